@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FLUPS solve path.
+
+Workload (one step = one solve): 512^3 cell-centred scalar Poisson on [0,1]^3,
+unbounded in all six faces, LGF_2 Green's kernel, transforms in FP32
+(FP64-computed twiddles, FP32 copy of the FP64 Green's spectrum); the RHS is a
+seeded sum of 8 Gaussians (synthetic).  The FP64 mode of the same solve is
+timed beside it and gives the FP32 error (relative L2 / Linf).
+
+Reported (one JSON line on rank 0):
+  value      grid points per second, input and output resident in HBM
+             (flups_solve on device pointers, CUDA events on the solver stream)
+  e2e        same metric through flups_solve with pinned host arrays
+             (H2D of the RHS and D2H of the field inside every step)
+  roofline   the dominant pass: algorithmic bytes per launch / its average
+             CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU oracle (numpy/scipy restatement of the reference
+             solver) on a bounded 128^3 sample, all host threads
+
+--impl reference times the reference's CPU algorithm (the oracle port: the
+reference needs FFTW, MPI and h3lpr, which this image does not have) on the
+same metric.  --gpus N runs N independent replicas (one per GPU): the solve
+does not shard.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "grid pts/s per solve FP32 vs FP64 at stated L2 err; %HBM roofline; p50/p99"
+UNIT = "grid pts/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--kernel", default="LGF_2")
+    ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
+    ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
+    return ap.parse_args()
+
+
+def rhs_gaussians(n, seed=2, device=None):
+    """Sum of 8 Gaussians, centres uniform in [0.2,0.8]^3, sigma in [0.03,0.08], amplitude in [-1,1]."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    if device is not None:
+        import torch
+        xs = torch.tensor(x, dtype=torch.float64, device=device)
+        out = torch.zeros((n, n, n), dtype=torch.float64, device=device)  # [z][y][x]
+        for _ in range(8):
+            c = rng.uniform(0.2, 0.8, 3)
+            s = rng.uniform(0.03, 0.08)
+            a = rng.uniform(-1, 1)
+            gx = torch.exp(-(xs - c[0]) ** 2 / s ** 2)
+            gy = torch.exp(-(xs - c[1]) ** 2 / s ** 2)
+            gz = torch.exp(-(xs - c[2]) ** 2 / s ** 2)
+            out += a * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]
+        return out
+    out = np.zeros((n, n, n))
+    for _ in range(8):
+        c = rng.uniform(0.2, 0.8, 3)
+        s = rng.uniform(0.03, 0.08)
+        a = rng.uniform(-1, 1)
+        gx = np.exp(-(x - c[0]) ** 2 / s ** 2)
+        gy = np.exp(-(x - c[1]) ** 2 / s ** 2)
+        gz = np.exp(-(x - c[2]) ** 2 / s ** 2)
+        out += a * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [v.strip() for v in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_oracle_sample(n, kernel, steps=3):
+    """Time the CPU oracle (FP64, all host threads) on an n^3 sample; returns pts/s and details."""
+    import scipy.fft as sfft
+
+    from oracle.plans import CELL_CENTER
+    from oracle.solver import OracleSolver
+    from flups_b200.pyflups import GreenType
+    ncores = os.cpu_count() or 1
+    o = OracleSolver([n] * 3, 1, [[[4], [4]]] * 3, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER)
+    o.green_type = int(GreenType[kernel])
+    o.setup()
+    rhs = rhs_gaussians(n)[None].transpose(0, 3, 2, 1).copy()
+    times = []
+    with sfft.set_workers(ncores):
+        o.solve(rhs)
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            o.solve(rhs)
+            times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    return n ** 3 / t, ncores, t
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = args.sample_n
+    pts, cores, t = None, None, None
+    times = []
+    import scipy.fft as sfft
+
+    from oracle.plans import CELL_CENTER
+    from oracle.solver import OracleSolver
+    from flups_b200.pyflups import GreenType
+    cores = os.cpu_count() or 1
+    o = OracleSolver([n] * 3, 1, [[[4], [4]]] * 3, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER)
+    o.green_type = int(GreenType[args.kernel])
+    o.setup()
+    rhs = rhs_gaussians(n)[None].transpose(0, 3, 2, 1).copy()
+    with sfft.set_workers(cores):
+        for _ in range(args.warmup):
+            o.solve(rhs)
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            o.solve(rhs)
+            times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = args.steps * n ** 3 / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian sum)",
+        "config": {"workload": f"{args.n}^3 cell-centred all-unbounded Poisson, {args.kernel}", "sample": f"{n}^3",
+                   "l2_flush": "host run"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n}^3 solves of the same workload (the reference's algorithm restated in numpy/scipy, FP64; FFTW/MPI absent here)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "p50_ms": float(np.percentile(times, 50) * 1e3), "p99_ms": float(np.percentile(times, 99) * 1e3),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def make_solver(pf, n, kernel, precision, stream):
+    B = pf.BoundaryType
+    t = pf.Topology(0, 1, [n, n, n])
+    s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1.0 / n] * 3, [1.0] * 3)
+    s.set_green_type(pf.GreenType[kernel])
+    s.set_precision(precision)
+    s.set_stream(stream)
+    t0 = time.perf_counter()
+    s.setup()
+    return t, s, time.perf_counter() - t0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    from flups_b200 import pyflups as pf
+    n = args.n
+    stream = torch.cuda.Stream(device=dev)
+    rhs = rhs_gaussians(n, device=dev)
+    field = torch.empty_like(rhs)
+
+    # ---------------------------------------------------------------- FP32 (headline)
+    t32, s32, setup32 = make_solver(pf, n, args.kernel, 32, stream)
+    s32.set_async(True)
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            s32.solve(field, rhs)
+    stream.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            s32.solve(field, rhs)
+            ev[k][1].record(stream)
+        t_all1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    elapsed = t_all0.elapsed_time(t_all1)  # ms
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        tt = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "ms_per_step": elapsed / args.steps, "n": n}), flush=True)
+        return
+    field32 = field.clone()
+
+    # per-pass device timing (separate short run) -> roofline of the dominant pass
+    s32.set_pass_timing(True)
+    with torch.cuda.stream(stream):
+        for _ in range(5):
+            s32.solve(field, rhs)
+    stream.synchronize()
+    stats = s32.pass_stats()
+    s32.set_pass_timing(False)
+    launches_per_solve = len(stats)
+    tot_bytes = sum(p["bytes"] for p in stats)
+    dom = max(stats, key=lambda p: p["ms_total"])
+    dom_ms = dom["ms_total"] / max(1, dom["calls"])
+    peak, peak_kind = measured_peaks()
+    achieved = dom["bytes"] / (dom_ms * 1e-3) / 1e9
+
+    # ---------------------------------------------------------------- e2e through the C ABI with host buffers
+    e2e_steps = min(args.steps, 5)
+    h_rhs = torch.empty((n, n, n), dtype=torch.float64, pin_memory=True)
+    h_rhs.copy_(rhs.cpu())
+    h_out = torch.empty_like(h_rhs).pin_memory()
+    s32.set_async(False)
+    s32.solve(h_out, h_rhs)  # warm the staging buffers
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        s32.solve(h_out, h_rhs)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    user_bytes = n ** 3 * 8
+
+    # ---------------------------------------------------------------- FP64 mode and the FP32 error
+    del s32, t32
+    torch.cuda.empty_cache()
+    t64, s64, setup64 = make_solver(pf, n, args.kernel, 64, stream)
+    s64.set_async(True)
+    field64 = torch.empty_like(rhs)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            s64.solve(field64, rhs)
+    stream.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    k64 = max(3, min(args.steps, 10))
+    f0.record(stream)
+    for _ in range(k64):
+        s64.solve(field64, rhs)
+    f1.record(stream)
+    f1.synchronize()
+    ms64 = f0.elapsed_time(f1) / k64
+    diff = field32 - field64
+    rel_l2 = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(field64))
+    rel_linf = float(diff.abs().max() / field64.abs().max())
+    del s64, t64
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    cpu_value, cores, cpu_t = cpu_oracle_sample(args.sample_n, args.kernel)
+    ms_per_step = elapsed / args.steps
+    value = world * n ** 3 / (ms_per_step * 1e-3)
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded sum of 8 Gaussians)",
+        "config": {"workload": f"{n}^3 cell-centred all-unbounded scalar Poisson, {args.kernel}, FP32 transforms",
+                   "grid": [n, n, n], "kernel": args.kernel, "l2_flush": "inputs larger than L2 (1 GiB RHS, 2+ GiB work arrays)",
+                   "parallelism": f"{world} independent replica(s)"},
+        "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+        "accuracy": {"fp32_rel_l2_vs_fp64": rel_l2, "fp32_rel_linf_vs_fp64": rel_linf,
+                     "fp64_pinned_to_oracle": "<=1e-12 rel L2 at 16^3-64^3 (tests/test_gpu_parity.py)"},
+        "fp64": {"value": world * n ** 3 / (ms64 * 1e-3), "ms_per_step": ms64},
+        "setup_s": {"fp32": setup32, "fp64": setup64},
+        "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": dom["bytes"], "ms_per_launch": dom_ms,
+                     "solve_bytes": tot_bytes, "solve_frac": tot_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+                     "passes": [{"name": p["name"], "ms": p["ms_total"] / max(1, p["calls"]), "bytes": p["bytes"]} for p in stats]},
+        "e2e": {"value": world * n ** 3 / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": user_bytes,
+                "d2h_bytes_per_step": user_bytes, "ms_per_step": e2e_ms},
+        "gpu_launches": launches_per_solve * args.steps,
+        "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.sample_n}^3 solves of the same workload, FP64 oracle (numpy/scipy restatement), median of 3"},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

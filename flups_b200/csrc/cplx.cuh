@@ -1,0 +1,131 @@
+// Small complex helpers and fixed-radix DFT butterflies (forward sign,
+// W_R = exp(-2 pi i / R)); inverse transforms conjugate on the way in and out.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace flb {
+
+template <typename T> struct CT;
+template <> struct CT<float> { using C = float2; };
+template <> struct CT<double> { using C = double2; };
+
+__device__ __forceinline__ float2 mkc(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 mkc(double x, double y) { return make_double2(x, y); }
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+    return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc(a.x, -a.y); }
+// a * (-i)
+template <typename C> __device__ __forceinline__ C cmul_mi(C a) { return mkc(a.y, -a.x); }
+template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) { return mkc(a.x * s, a.y * s); }
+
+template <typename C> __device__ __forceinline__ void dft2(C* v) {
+    C t = v[0];
+    v[0] = cadd(t, v[1]);
+    v[1] = csub(t, v[1]);
+}
+
+template <typename C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
+    C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    C t2 = cadd(a1, a3), t3 = cmul_mi(csub(a1, a3));
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, t3);
+    a3 = csub(t1, t3);
+}
+template <typename C> __device__ __forceinline__ void dft4(C* v) { dft4(v[0], v[1], v[2], v[3]); }
+
+// sqrt(1/2), cos(pi/8), sin(pi/8)
+#define FLB_R2 0.70710678118654752440
+#define FLB_C8 0.92387953251128675613
+#define FLB_S8 0.38268343236508977173
+
+template <typename C> __device__ __forceinline__ void dft8(C* v) {
+    using S = decltype(v[0].x);
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4(e0, e1, e2, e3);
+    dft4(o0, o1, o2, o3);
+    const S r2 = (S)FLB_R2;
+    o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);  // * W8^1
+    o2 = cmul_mi(o2);                                   // * W8^2
+    o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // * W8^3
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+// W16^m = (cos(pi m/8), -sin(pi m/8)), m in 0..9
+template <typename S> __device__ __forceinline__ void w16(int m, S& c, S& s) {
+    switch (m) {
+        case 0: c = (S)1; s = (S)0; break;
+        case 1: c = (S)FLB_C8; s = -(S)FLB_S8; break;
+        case 2: c = (S)FLB_R2; s = -(S)FLB_R2; break;
+        case 3: c = (S)FLB_S8; s = -(S)FLB_C8; break;
+        case 4: c = (S)0; s = (S)-1; break;
+        case 6: c = -(S)FLB_R2; s = -(S)FLB_R2; break;
+        case 9: c = -(S)FLB_C8; s = (S)FLB_S8; break;
+        default: c = (S)0; s = (S)0; break;
+    }
+}
+
+template <typename C> __device__ __forceinline__ void dft16(C* v) {
+    using S = decltype(v[0].x);
+    // inner DFT4 over j1 of a[j2 + 4 j1], twiddle W16^{j2 k1}, outer DFT4 over j2
+#pragma unroll
+    for (int j2 = 0; j2 < 4; ++j2) dft4(v[j2], v[j2 + 4], v[j2 + 8], v[j2 + 12]);
+#pragma unroll
+    for (int j2 = 1; j2 < 4; ++j2) {
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) {
+            S c, s;
+            w16<S>(j2 * k1, c, s);
+            v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, s));
+        }
+    }
+    C t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        C a0 = v[0 + 4 * k1], a1 = v[1 + 4 * k1], a2 = v[2 + 4 * k1], a3 = v[3 + 4 * k1];
+        dft4(a0, a1, a2, a3);
+        t[k1 + 0] = a0; t[k1 + 4] = a1; t[k1 + 8] = a2; t[k1 + 12] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+template <typename C> __device__ __forceinline__ void dft3(C* v) {
+    using S = decltype(v[0].x);
+    const S h = (S)0.5, s3 = (S)0.86602540378443864676;
+    C a = cadd(v[1], v[2]);
+    C d = cmul_mi(csub(v[1], v[2]));
+    C t = csub(v[0], cscale(a, h));
+    v[0] = cadd(v[0], a);
+    C u = cscale(d, s3);
+    v[1] = cadd(t, u);
+    v[2] = csub(t, u);
+}
+
+template <typename C> __device__ __forceinline__ void dft5(C* v) {
+    using S = decltype(v[0].x);
+    const S c1 = (S)0.30901699437494742410, c2 = (S)-0.80901699437494742410;
+    const S s1 = (S)0.95105651629515357212, s2 = (S)0.58778525229247312917;
+    C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    C x0 = v[0];
+    v[0] = cadd(x0, cadd(a1, a2));
+    C p1 = cadd(x0, cadd(cscale(a1, c1), cscale(a2, c2)));
+    C q1 = cmul_mi(cadd(cscale(b1, s1), cscale(b2, s2)));
+    C p2 = cadd(x0, cadd(cscale(a1, c2), cscale(a2, c1)));
+    C q2 = cmul_mi(csub(cscale(b1, s2), cscale(b2, s1)));
+    v[1] = cadd(p1, q1);
+    v[4] = csub(p1, q1);
+    v[2] = cadd(p2, q2);
+    v[3] = csub(p2, q2);
+}
+
+}  // namespace flb

@@ -1,0 +1,175 @@
+// Host-side layout, plan tables and solver of the B200 FLUPS library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/flups.h"
+#include "green.cuh"
+#include "pass_desc.h"
+
+#define FLB_CHECK(cond, ...)                                                        \
+    do {                                                                            \
+        if (!(cond)) {                                                              \
+            fprintf(stderr, "[flups_b200] error in %s: ", __func__);               \
+            fprintf(stderr, __VA_ARGS__);                                           \
+            fprintf(stderr, "\n");                                                  \
+            fflush(stderr);                                                         \
+            abort();                                                                \
+        }                                                                           \
+    } while (0)
+
+namespace flb {
+
+cudaError_t launch_line_pass(const PassArgs& A, int compute_f64, int in_f64, int out_f64, cudaStream_t stream);
+size_t line_pass_smem(const PassArgs& A, int elem_bytes);
+cudaError_t launch_green_eval(const GreenEvalArgs& A, cudaStream_t s);
+cudaError_t launch_green_final(const GreenFinalArgs& A, cudaStream_t s);
+
+// plan types and FFTW r2r kinds (src/FFTW_plan_dim.hpp:34-62)
+enum PlanType { SYMSYM = 2, MIXUNB = 5, PERPER = 6, UNBUNB = 8, EMPTY = 18 };
+enum R2RKind { K_NONE = 0, REDFT00, REDFT10, REDFT01, REDFT11, RODFT00, RODFT10, RODFT01, RODFT11 };
+
+// One direction's transform: a restatement of the tables of FFTW_plan_dim
+// (src/FFTW_plan_dim.cpp:77-161) and of its cell/node initialisers
+// (src/FFTW_plan_dim_cell.cpp:19-390, src/FFTW_plan_dim_node.cpp:19-461).
+struct DirPlan {
+    int lda = 1, dim = 0, sign = FLUPS_FORWARD;
+    bool is_green = false;
+    int center = CELL_CENTER;
+    int bc[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    int type = EMPTY;
+    double volfact = 1.0, kfact = 0.0, normfact = 1.0, symstart = 0.0, koffset = 0.0;
+    bool is_spectral = false, isr2c = false;
+    int n_in[3] = {1, 1, 1}, fstart_in[3] = {0, 0, 0}, fstart_out[3] = {0, 0, 0}, postpro[3] = {0, 0, 0};
+    bool imult[3] = {false, false, false};
+    int kind[3] = {K_NONE, K_NONE, K_NONE};
+    int n_out = 1, fieldstart = 0;
+
+    DirPlan() = default;
+    DirPlan(int lda, int dim, const double h[3], const double L[3], const int bcl[3], const int bcr[3], int sign, bool green,
+            int center);
+    bool isr2c_done_by_fft() const { return isr2c && !is_spectral; }
+    void init(const int size[3], bool is_complex);
+
+   private:
+    void r2r_cell(int n);
+    void mix_cell(int n);
+    void per_cell(int n, bool c);
+    void unb_cell(int n, bool c);
+    void r2r_node(int n);
+    void mix_node(int n);
+    void per_node(int n, bool c);
+    void unb_node(int n, bool c);
+};
+
+void sort_plans(DirPlan p[3]);
+
+}  // namespace flb
+
+// Opaque handles of the C API
+struct Topology {
+    int axis = 0, lda = 1, nf = 1, alignment = FLUPS_ALIGNMENT;
+    int nglob[3] = {1, 1, 1}, nloc[3] = {1, 1, 1}, nmem[3] = {1, 1, 1}, nproc[3] = {1, 1, 1}, axproc[3] = {0, 1, 2};
+    MPI_Comm comm = 0;
+    void cmpt_sizes();  // src/Topology.cpp:81-98
+    size_t memdim() const { return (size_t)nmem[0] * nmem[1] * nmem[2] * nf; }
+    size_t memsize() const { return memdim() * lda; }
+    size_t locsize() const { return (size_t)nloc[0] * nloc[1] * nloc[2] * nf; }
+};
+
+struct Profiler {
+    std::string name;
+    std::map<std::string, double> acc_ms;
+    std::map<std::string, long> count;
+};
+
+// Array state between passes: extents along x, y, z and element type.
+struct ArrState {
+    int n[3];
+    bool cplx;
+};
+
+struct Solver {
+    // ---------------------------------------------------------------- inputs
+    Topology* topo_phys = nullptr;
+    int lda = 1;
+    double h[3] = {1, 1, 1}, L[3] = {1, 1, 1};
+    int odiff = NOD;
+    int center = CELL_CENTER;
+    int bc[3][2][3];
+    int green_type = CHAT_2;
+    double alpha = 2.0;
+    int precision = 64;
+    bool async = false;
+    bool skip_st0 = false;
+    cudaStream_t stream = 0;
+    Profiler* prof = nullptr;
+    int last_error = 0;
+    // ---------------------------------------------------------------- plans
+    flb::DirPlan fwd[3], bwd[3], grn[3], dif[3];
+    bool have_diff = false;
+    int ndim = 3;
+    double normfact = 1.0, volfact = 1.0;
+    ArrState st[4];            // st[k]: array after k forward transforms
+    int sizes_before[3][3];    // size before forward plan ip
+    // ---------------------------------------------------------------- device data
+    bool is_setup = false;
+    void* buf[2] = {nullptr, nullptr};    // work arrays (working precision)
+    size_t buf_elems[2] = {0, 0};         // capacity in reals
+    int buf_batch = 0;
+    void* green = nullptr;                // folded Green's spectrum (working precision)
+    int gfold_M[3] = {0, 0, 0}, gfold_n[3] = {1, 1, 1};
+    int64_t gstr[3] = {1, 1, 1};
+    std::map<int64_t, void*> twiddles;    // key: M * 2 + (precision == 64)
+    double* stage_in = nullptr;           // device staging for host rhs/field
+    size_t stage_elems = 0;
+    double* inner = nullptr;              // spectral buffer of the advanced API (doubles)
+    Topology* topo_spec = nullptr;
+    Topology* topo_inner_phys = nullptr;
+    // ---------------------------------------------------------------- host-only planning
+    bool dry = false;                     // record passes instead of launching them
+    std::vector<flb::PassArgs> dry_passes;
+    std::vector<int> dry_flags;
+    std::vector<std::string> dry_names;
+    // ---------------------------------------------------------------- per-pass timing
+    bool timing = false;
+    int pass_idx = 0;
+    std::vector<cudaEvent_t> ev;          // 2 per pass of the last solve
+    std::vector<double> pass_ms, pass_bytes;
+    std::vector<long> pass_calls;
+    std::vector<std::string> pass_names;
+
+    Solver(Topology* t, FLUPS_BoundaryType* bc[3][2], const double h[3], const double L[3], int odiff, const int center[3],
+           Profiler* prof);
+    ~Solver();
+    void setup();
+    void solve(double* field, double* rhs, int type, int nbatch);
+    size_t alloc_size() const;
+    size_t device_bytes(int nbatch) const;
+    void spectral_info(double kfact[3], double koffset[3], double symstart[3]) const;
+
+    // ---------------------------------------------------------------- internals
+    void dry_run(flb::DirPlan p[3]);
+    void compute_green();
+    const void* twiddle(int M, bool f64);
+    void ensure_buffers(int nbatch);
+    flb::LineStage stage_forward(const flb::DirPlan& p, int ip, bool f64);
+    flb::LineStage stage_backward(const flb::DirPlan& p, const flb::DirPlan& pf, int ip, bool f64);
+    flb::PassArgs base_pass(int axis, const ArrState& src, int ncomp, int lda_spec);
+    void set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s) const;
+    void set_strides_user(int64_t str[3], int64_t& cstr) const;
+    void fit_lines(flb::PassArgs& A, int elem_bytes) const;
+    flb::MultSpec mult_spec(int type) const;
+    void run_pass(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64, const char* name = "pass");
+    void collect_timing();
+    void check_cuda(cudaError_t e, const char* what);
+    void do_fft_forward(const double* user_in, int nbatch);
+    void do_fft_backward_fused(double* user_out, int type, int nbatch);
+    std::string plan_json(int type, int nbatch);
+};

@@ -1,0 +1,904 @@
+// Solver orchestration: plans, Green's function setup, and the pass sequence
+// of one solve.  Reference: src/Solver.cpp:23-202 (ctor and dry run),
+// :219-469 (setup), :980-1154 (Green's function), :1207-1272 (solve),
+// :1402-1542 (do_FFT / do_mult).
+//
+// Device data layout (every array x fastest, then y, then z, then component
+// or batch):
+//   state k = the field after the first k forward transforms; its extents are
+//   the reference's topo_hat_[k-1] sizes, stored x fastest instead of
+//   pencil-major, so no transpose is ever materialised.
+//   Pass sequence for ndim directions: fwd 0 .. fwd ndim-2, one fused pass
+//   (fwd ndim-1, Green multiply, bwd ndim-1) in place, bwd ndim-2 .. bwd 0.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "host.hpp"
+
+using namespace flb;
+
+namespace flb {
+int load_lgf_table(int kind, int ndim, std::vector<double>& data);
+int farfield_terms(int kind, int ndim, std::vector<FarTerm>& terms, double& logc);
+}  // namespace flb
+
+static int r2r_to_line(int k) {
+    switch (k) {
+        case REDFT00: return LK_DCT1;
+        case REDFT10: return LK_DCT2;
+        case REDFT01: return LK_DCT3;
+        case REDFT11: return LK_DCT4;
+        case RODFT00: return LK_DST1;
+        case RODFT10: return LK_DST2;
+        case RODFT01: return LK_DST3;
+        case RODFT11: return LK_DST4;
+    }
+    return LK_NONE;
+}
+
+static int fft_length(int kind, int n) {
+    switch (kind) {
+        case LK_DCT1: return 2 * (n - 1);
+        case LK_DST1: return 2 * (n + 1);
+        case LK_DCT2: case LK_DCT3: case LK_DCT4: case LK_DST2: case LK_DST3: case LK_DST4: return 2 * n;
+        default: return n;
+    }
+}
+
+static void factorize(int M, LineStage& S) {
+    S.nrad = 0;
+    int m = M;
+    const int pref[4] = {16, 8, 4, 2};
+    for (int r : pref) {
+        while (m % r == 0 && m > 1) {
+            FLB_CHECK(S.nrad < kMaxRadices, "too many FFT stages");
+            S.radix[S.nrad++] = r;
+            m /= r;
+        }
+    }
+    for (int p = 3; m > 1; p += 2) {
+        while (m % p == 0) {
+            FLB_CHECK(p <= 64, "transform length %d has a prime factor %d > 64 (not supported)", M, p);
+            FLB_CHECK(S.nrad < kMaxRadices, "too many FFT stages");
+            S.radix[S.nrad++] = p;
+            m /= p;
+        }
+    }
+    if (S.nrad == 0) S.radix[S.nrad++] = 1;
+}
+
+// ---------------------------------------------------------------------------
+Solver::Solver(Topology* t, FLUPS_BoundaryType* bcin[3][2], const double hin[3], const double Lin[3], int od, const int ctr[3],
+               Profiler* p)
+    : topo_phys(t), odiff(od), prof(p) {
+    FLB_CHECK(t != nullptr, "topology is NULL");
+    FLB_CHECK(t->nproc[0] * t->nproc[1] * t->nproc[2] == 1, "this library runs on a size-1 communicator");
+    FLB_CHECK(!t->nf || t->nf == 1, "The RHS topology cannot be complex");
+    FLB_CHECK(ctr[0] == ctr[1] && ctr[0] == ctr[2], "We handle only data located at the same place in all the direction");
+    lda = t->lda;
+    FLB_CHECK(lda >= 1 && lda <= 3, "lda must be 1, 2 or 3");
+    center = ctr[0];
+    for (int d = 0; d < 3; ++d) {
+        h[d] = hin[d];
+        L[d] = Lin[d];
+        for (int s = 0; s < 2; ++s)
+            for (int c = 0; c < lda; ++c) bc[d][s][c] = bcin[d][s][c];
+    }
+    for (int d = 0; d < 3; ++d) {
+        fwd[d] = DirPlan(lda, d, h, L, bc[d][0], bc[d][1], FLUPS_FORWARD, false, center);
+        bwd[d] = DirPlan(lda, d, h, L, bc[d][0], bc[d][1], FLUPS_BACKWARD, false, center);
+        grn[d] = DirPlan(1, d, h, L, bc[d][0], bc[d][1], FLUPS_FORWARD, true, center);
+    }
+    sort_plans(fwd);
+    sort_plans(bwd);
+    sort_plans(grn);
+    if (odiff != NOD) {
+        // Solver.cpp:86-143: backward plans of the derivative swap EVEN and ODD
+        have_diff = true;
+        for (int id = 0; id < 3; ++id) {
+            const int d = bwd[id].dim;
+            int l[3], r[3];
+            for (int c = 0; c < lda; ++c) {
+                auto sw = [](int b) { return b == EVEN ? ODD : (b == ODD ? EVEN : b); };
+                l[c] = sw(bc[d][0][c]);
+                r[c] = sw(bc[d][1][c]);
+            }
+            dif[id] = DirPlan(lda, d, h, L, l, r, FLUPS_BACKWARD, false, center);
+        }
+    }
+    ndim = 0;
+    for (int d = 0; d < 3; ++d)
+        if (fwd[d].type != EMPTY) ++ndim;
+    FLB_CHECK(ndim > 1, "We only hanlde 2D and 3D field");
+    dry_run(fwd);
+    {
+        // states of the field after each forward transform
+        st[0].cplx = false;
+        for (int d = 0; d < 3; ++d) st[0].n[d] = t->nglob[d];
+        for (int ip = 0; ip < ndim; ++ip) {
+            st[ip + 1] = st[ip];
+            st[ip + 1].n[fwd[ip].dim] = fwd[ip].n_out;
+            st[ip + 1].cplx = st[ip].cplx || fwd[ip].isr2c;
+        }
+    }
+    dry_run(bwd);
+    dry_run(grn);
+    if (have_diff) dry_run(dif);
+    normfact = 1.0;
+    volfact = 1.0;
+    for (int ip = 0; ip < 3; ++ip) {
+        normfact *= fwd[ip].normfact;
+        volfact *= fwd[ip].volfact;
+    }
+}
+
+void Solver::dry_run(DirPlan p[3]) {
+    // Solver.cpp:617-650
+    int size[3] = {topo_phys->nglob[0], topo_phys->nglob[1], topo_phys->nglob[2]};
+    bool cplx = false;
+    for (int ip = 0; ip < ndim; ++ip) {
+        if (&p[0] == &fwd[0])
+            for (int d = 0; d < 3; ++d) sizes_before[ip][d] = size[d];
+        p[ip].init(size, cplx);
+        size[p[ip].dim] = p[ip].n_out;
+        cplx = cplx || p[ip].isr2c;
+    }
+}
+
+Solver::~Solver() {
+    for (auto& b : buf)
+        if (b) cudaFree(b);
+    if (green) cudaFree(green);
+    for (auto& kv : twiddles) cudaFree(kv.second);
+    if (stage_in) cudaFree(stage_in);
+    if (inner) cudaFree(inner);
+    for (auto e : ev) cudaEventDestroy(e);
+    delete topo_spec;
+    delete topo_inner_phys;
+}
+
+void Solver::check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        last_error = (int)e;
+        FLB_CHECK(false, "CUDA error during %s: %s", what, cudaGetErrorString(e));
+    }
+}
+
+void Solver::spectral_info(double kf[3], double ko[3], double ss[3]) const {
+    // Solver.hpp:222-229
+    for (int ip = 0; ip < 3; ++ip) {
+        const int d = fwd[ip].dim;
+        kf[d] = fwd[ip].kfact;
+        ss[d] = fwd[ip].symstart;
+        ko[d] = fwd[ip].koffset;
+    }
+}
+
+size_t Solver::alloc_size() const {
+    size_t m = 1;
+    for (int k = 1; k <= ndim; ++k) {
+        size_t e = (size_t)st[k].n[0] * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda;
+        m = std::max(m, e);
+    }
+    return std::max(m, topo_phys->memsize());
+}
+
+const void* Solver::twiddle(int M, bool f64) {
+    const int64_t key = (int64_t)M * 2 + (f64 ? 1 : 0);
+    auto it = twiddles.find(key);
+    if (it != twiddles.end()) return it->second;
+    // W_{2M}^q = exp(-2 pi i q / (2M)), q in [0, 2M), evaluated in FP64
+    std::vector<double> w(4 * (size_t)M);
+    for (int q = 0; q < 2 * M; ++q) {
+        // reduce to the first quadrant for accuracy: angle = -pi q / M
+        const long double a = -(long double)M_PI * (long double)q / (long double)M;
+        w[2 * q] = (double)cosl(a);
+        w[2 * q + 1] = (double)sinl(a);
+    }
+    void* d = nullptr;
+    if (f64) {
+        check_cuda(cudaMalloc(&d, w.size() * sizeof(double)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice), "twiddle upload");
+    } else {
+        std::vector<float> wf(w.size());
+        for (size_t i = 0; i < w.size(); ++i) wf[i] = (float)w[i];
+        check_cuda(cudaMalloc(&d, wf.size() * sizeof(float)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice), "twiddle upload");
+    }
+    twiddles[key] = d;
+    return d;
+}
+
+// ---------------------------------------------------------------- stages
+LineStage Solver::stage_forward(const DirPlan& p, int ip, bool f64) {
+    LineStage S;
+    memset(&S, 0, sizeof(S));
+    int M = -1;
+    for (int c = 0; c < p.lda; ++c) {
+        LineSpec& sp = S.spec[c];
+        if (p.type == SYMSYM || p.type == MIXUNB) {
+            sp.kind = r2r_to_line(p.kind[c]);
+            sp.n_in = p.n_in[c];
+        } else {
+            sp.kind = p.isr2c ? LK_R2C : LK_C2C;
+            sp.n_in = p.n_in[0];
+        }
+        sp.sign = -1;
+        sp.fi = p.fstart_in[c];
+        sp.fo = p.fstart_out[c];
+        sp.postpro = p.postpro[c];
+        sp.nfftw = p.n_out - 1;
+        const int m = fft_length(sp.kind, sp.n_in);
+        FLB_CHECK(M < 0 || M == m, "components need transforms of the same length");
+        M = m;
+    }
+    for (int c = p.lda; c < kMaxComp; ++c) S.spec[c] = S.spec[0];
+    S.M = M;
+    factorize(M, S);
+    S.n_b = p.isr2c ? 2 * p.n_out : p.n_out;
+    S.fieldstart = p.fieldstart;
+    S.n_o = p.n_out;
+    S.in_cplx = (ip >= 0) ? st[ip].cplx : 0;
+    S.out_cplx = (ip >= 0) ? st[ip + 1].cplx : 0;
+    S.store_off = 0;
+    S.n_store = S.n_o;
+    S.tw = nullptr;  // resolved at launch
+    return S;
+}
+
+LineStage Solver::stage_backward(const DirPlan& p, const DirPlan& pf, int ip, bool f64) {
+    LineStage S;
+    memset(&S, 0, sizeof(S));
+    int M = -1;
+    for (int c = 0; c < p.lda; ++c) {
+        LineSpec& sp = S.spec[c];
+        if (p.type == SYMSYM || p.type == MIXUNB) {
+            sp.kind = r2r_to_line(p.kind[c]);
+            sp.n_in = p.n_in[c];
+        } else {
+            sp.kind = pf.isr2c ? LK_C2R : LK_C2C;
+            sp.n_in = p.n_in[0];
+        }
+        sp.sign = +1;
+        sp.fi = p.fstart_in[c];
+        sp.fo = p.fstart_out[c];
+        sp.postpro = p.postpro[c];
+        sp.nfftw = p.n_in[c];
+        const int m = fft_length(sp.kind, sp.n_in);
+        FLB_CHECK(M < 0 || M == m, "components need transforms of the same length");
+        M = m;
+    }
+    for (int c = p.lda; c < kMaxComp; ++c) S.spec[c] = S.spec[0];
+    S.M = M;
+    factorize(M, S);
+    S.n_b = p.n_out;
+    S.fieldstart = 0;
+    S.n_o = pf.isr2c ? 2 * p.n_out : p.n_out;
+    S.in_cplx = st[ip + 1].cplx;
+    S.out_cplx = st[ip].cplx;
+    S.store_off = pf.fieldstart;
+    S.n_store = st[ip].n[pf.dim];
+    S.tw = nullptr;  // resolved at launch
+    return S;
+}
+
+void Solver::set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s) const {
+    str[0] = 1;
+    str[1] = s.n[0];
+    str[2] = (int64_t)s.n[0] * s.n[1];
+    cstr = (int64_t)s.n[0] * s.n[1] * s.n[2];
+}
+
+void Solver::set_strides_user(int64_t str[3], int64_t& cstr) const {
+    // flups_locID layout of the user topology (src/flups.h:109-119)
+    const Topology* t = topo_phys;
+    const int a0 = t->axis, a1 = (a0 + 1) % 3, a2 = (a0 + 2) % 3;
+    str[a0] = 1;
+    str[a1] = t->nmem[a0];
+    str[a2] = (int64_t)t->nmem[a0] * t->nmem[a1];
+    cstr = (int64_t)t->memdim();
+}
+
+PassArgs Solver::base_pass(int axis, const ArrState& src, int ncomp, int lda_spec) {
+    PassArgs A;
+    memset(&A, 0, sizeof(A));
+    A.axis = axis;
+    A.n_src = src.n[axis];
+    const int a = (axis == 0) ? 1 : 0, b = (axis == 2) ? 1 : 2;
+    A.n_a = src.n[a];
+    A.n_b = src.n[b];
+    A.nlines = A.n_a * A.n_b;
+    A.ncomp = ncomp;
+    A.lda = lda_spec;
+    return A;
+}
+
+void Solver::fit_lines(PassArgs& A, int elem_bytes) const {
+    A.lines_per_cta = 1;
+    const size_t one = line_pass_smem(A, elem_bytes);
+    FLB_CHECK(one <= 227 * 1024, "a line of this size does not fit in shared memory (%zu bytes)", one);
+    int tl = (int)std::min<size_t>(32, (200 * 1024) / one);
+    tl = std::max(tl, 1);
+    const int64_t work = A.comps_together ? A.nlines : (int64_t)A.nlines * A.ncomp;
+    if (tl > work) tl = (int)std::max<int64_t>(1, work);
+    A.lines_per_cta = tl;
+}
+
+MultSpec Solver::mult_spec(int type) const {
+    MultSpec G;
+    memset(&G, 0, sizeof(G));
+    G.mode = (type == ROT) ? 2 : 1;
+    G.green = green;
+    for (int d = 0; d < 3; ++d) {
+        G.gstr[d] = gstr[d];
+        G.gfold[d] = gfold_M[d];
+        G.gn[d] = gfold_n[d];
+        G.hgrid[d] = h[d];
+    }
+    G.normfact = normfact;
+    G.odiff = odiff;
+    if (type == ROT) {
+        double kabs[3], ko[3], ss[3];
+        spectral_info(kabs, ko, ss);
+        for (int d = 0; d < 3; ++d) {
+            G.koffset[d] = ko[d];
+            G.symstart[d] = ss[d];
+        }
+        // Solver.cpp:1485-1516: phase of the derivative from the forward and backward-diff imult
+        for (int ip = 0; ip < 3; ++ip) {
+            const int d = fwd[ip].dim;
+            for (int c = 0; c < 3; ++c) {
+                const int cc = c < lda ? c : 0;
+                int ph = 0;
+                if (fwd[ip].imult[cc]) ph--;
+                if (dif[ip].imult[cc]) ph++;
+                if (ph == 0) { G.kfact[d][c][0] = 0.0; G.kfact[d][c][1] = kabs[d]; }
+                else if (ph == 1) { G.kfact[d][c][0] = -kabs[d]; G.kfact[d][c][1] = 0.0; }
+                else { G.kfact[d][c][0] = kabs[d]; G.kfact[d][c][1] = 0.0; }
+            }
+        }
+    }
+    return G;
+}
+
+void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, const char* name) {
+    PassArgs A = Ain;
+    if (dry) {
+        dry_passes.push_back(A);
+        dry_flags.push_back((f64 ? 1 : 0) | (in_f64 ? 2 : 0) | (out_f64 ? 4 : 0));
+        dry_names.push_back(name);
+        return;
+    }
+    for (int s2 = 0; s2 <= A.fused; ++s2)
+        if (!A.st[s2].tw) A.st[s2].tw = twiddle(A.st[s2].M, f64);
+    const int k = pass_idx++;
+    if (timing) {
+        // algorithmic bytes: source and kept output lines once, the folded Green's spectrum once
+        const int64_t nc = A.comps_together ? (int64_t)A.ncomp : (int64_t)A.ncomp;
+        const double es = f64 ? 8.0 : 4.0;
+        const LineStage& last = A.st[A.fused ? 1 : 0];
+        double bytes = (double)A.n_src * A.nlines * nc * (A.st[0].in_cplx ? 2 : 1) * (in_f64 ? 8.0 : 4.0) +
+                       (double)last.n_store * A.nlines * nc * (last.out_cplx ? 2 : 1) * (out_f64 ? 8.0 : 4.0);
+        if (A.fused) bytes += (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
+        if ((int)pass_ms.size() <= k) {
+            pass_ms.resize(k + 1, 0.0);
+            pass_bytes.resize(k + 1, 0.0);
+            pass_calls.resize(k + 1, 0);
+            pass_names.resize(k + 1);
+        }
+        pass_bytes[k] = bytes;
+        pass_names[k] = name;
+        while ((int)ev.size() < 2 * (k + 1)) {
+            cudaEvent_t e;
+            check_cuda(cudaEventCreate(&e), "event");
+            ev.push_back(e);
+        }
+        cudaEventRecord(ev[2 * k], stream);
+    }
+    check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
+    if (timing) cudaEventRecord(ev[2 * k + 1], stream);
+}
+
+void Solver::collect_timing() {
+    if (!timing) return;
+    check_cuda(cudaEventSynchronize(ev[2 * (pass_idx - 1) + 1]), "timing");
+    for (int k = 0; k < pass_idx; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+        pass_ms[k] += ms;
+        pass_calls[k] += 1;
+    }
+}
+
+// ---------------------------------------------------------------- Green
+void Solver::compute_green() {
+    // Solver.cpp:980-1106
+    const int kind = green_type;
+    double length = alpha * h[0];
+    if (kind == HEJ_0) length = h[0] / M_PI;
+    const bool iso_kernel = (kind == HEJ_2 || kind == HEJ_4 || kind == HEJ_6 || kind == HEJ_8 || kind == HEJ_10 || kind == HEJ_0 ||
+                             kind == LGF_2);
+    FLB_CHECK(!(iso_kernel && ((ndim == 3 && (h[0] != h[1] || h[1] != h[2])) || (ndim == 2 && h[0] != h[1]))),
+              "You are trying to use a regularized kernel or a LGF while not having dx=dy=dz.");
+    const bool is_hej = (kind == HEJ_2 || kind == HEJ_4 || kind == HEJ_6 || kind == HEJ_8 || kind == HEJ_10);
+    const bool is_lgf = (kind == LGF_2 || kind == LGF_4 || kind == LGF_6 || kind == LGF_8);
+    const bool is_meh = (kind == MEHR_4L || kind == MEHR_4F || kind == MEHR_6L || kind == MEHR_6F);
+
+    bool spec[3] = {false, false, false};
+    double symstart[3] = {0, 0, 0}, hfact[3] = {0, 0, 0}, kfact[3] = {0, 0, 0}, koffset[3] = {0, 0, 0};
+    for (int ip = 0; ip < ndim; ++ip) {
+        const DirPlan& p = grn[ip];
+        const int d = p.dim;
+        spec[d] = p.is_spectral;
+        symstart[d] = p.symstart;
+        hfact[d] = h[d];
+        if (p.is_spectral) {
+            hfact[d] = 0.0;
+            kfact[d] = p.kfact;
+            koffset[d] = p.koffset;
+        }
+        if (p.type == EMPTY) hfact[d] = 0.0;
+    }
+    int nspec = 0;
+    for (int d = 0; d < ndim; ++d)
+        if (spec[d]) ++nspec;
+    const int nunb = ndim - nspec;
+
+    // spectral extents of the Green's function and its topology 0 (Solver.cpp:727-781)
+    int spec_n[3] = {topo_phys->nglob[0], topo_phys->nglob[1], topo_phys->nglob[2]};
+    bool spec_cplx = false;
+    for (int ip = 0; ip < ndim; ++ip) {
+        spec_n[grn[ip].dim] = grn[ip].n_out;
+        spec_cplx = spec_cplx || grn[ip].isr2c;
+    }
+    int size0[3] = {spec_n[0], spec_n[1], spec_n[2]};
+    bool cplx0 = spec_cplx;
+    for (int ip = ndim - 1; ip >= 0; --ip)
+        if (grn[ip].isr2c_done_by_fft()) {
+            size0[grn[ip].dim] *= 2;
+            cplx0 = false;
+        }
+    const size_t n0 = (size_t)size0[0] * size0[1] * size0[2] * (cplx0 ? 2 : 1);
+    const size_t ns = (size_t)spec_n[0] * spec_n[1] * spec_n[2] * (spec_cplx ? 2 : 1);
+    size_t nmax = std::max(n0, ns);
+    // intermediate states are never larger than max(start, end) along each transformed direction
+    double* gb[2] = {nullptr, nullptr};
+    if (!dry) {
+        // every intermediate state holds at most nmax doubles (each pass keeps or halves/doubles
+        // the real count of one direction between the two ends)
+        check_cuda(cudaMalloc(&gb[0], nmax * sizeof(double)), "Green buffer");
+        check_cuda(cudaMalloc(&gb[1], nmax * sizeof(double)), "Green buffer");
+    }
+
+    GreenEvalArgs E;
+    memset(&E, 0, sizeof(E));
+    E.kind = kind;
+    E.nunb = nunb;
+    for (int d = 0; d < 3; ++d) {
+        E.size[d] = size0[d];
+        E.symstart[d] = symstart[d];
+        E.hfact[d] = hfact[d];
+        E.kfact[d] = kfact[d];
+        E.koffset[d] = koffset[d];
+    }
+    E.cplx = cplx0;
+    const int ax0 = grn[0].dim;
+    E.ax[0] = ax0;
+    E.ax[1] = (ax0 + 1) % 3;
+    E.ax[2] = (ax0 + 2) % 3;
+    E.length = length;
+    std::vector<double> table;
+    std::vector<FarTerm> far;
+    double far_log = 0.0;
+    double* d_table = nullptr;
+    FarTerm* d_far = nullptr;
+    if (nunb == 3) {
+        E.hgrid = hfact[E.ax[0]];
+        if (is_lgf || is_meh) {
+            E.tableN = load_lgf_table(kind, 3, table);
+            farfield_terms(kind, 3, far, far_log);
+        } else {
+            E.set_g0 = 1;
+            const double s3 = std::sqrt(M_PI * M_PI * M_PI);
+            const double r2 = std::sqrt(2.0);
+            switch (kind) {
+                case HEJ_2: E.g0 = -r2 / (4.0 * length * s3); break;
+                case HEJ_4: E.g0 = -3.0 * r2 / (8.0 * length * s3); break;
+                case HEJ_6: E.g0 = -15.0 * r2 / (32.0 * length * s3); break;
+                case HEJ_8: E.g0 = -35.0 * r2 / (64.0 * length * s3); break;
+                case HEJ_10: E.g0 = -315.0 * r2 / (512.0 * length * s3); break;
+                case HEJ_0: E.g0 = -1.0 / (2.0 * M_PI * M_PI * length); break;
+                case CHAT_2: {
+                    const double hp = hfact[0] * hfact[1] * hfact[2];
+                    E.g0 = -0.5 * std::pow(1.5 * (1.0 / (2.0 * M_PI)) * hp, 2. / 3.) / hp;
+                    break;
+                }
+                default: FLB_CHECK(false, "Green Function type unknown.");
+            }
+        }
+    } else if (nunb == 2) {
+        const double ha = hfact[E.ax[0]], hb = hfact[E.ax[1]], hc = hfact[E.ax[2]];
+        E.r_eq2d = (1.0 / std::sqrt(M_PI)) * std::sqrt(ha * hb + hb * hc + hc * ha);
+        E.r_cut = (ha + hb + hc) * .2;
+        E.k_cut = (kfact[E.ax[0]] + kfact[E.ax[1]] + kfact[E.ax[2]]) * 0.2;
+        E.chat2d_origin = (kind == CHAT_2);
+        if (is_lgf || is_meh) {
+            E.tableN = load_lgf_table(kind, 2, table);
+            farfield_terms(kind, 2, far, far_log);
+        }
+    } else if (nunb == 1) {
+        FLB_CHECK(kind != HEJ_0, "HEJ0 kernel not available for 1D unbounded problems.");
+        FLB_CHECK(is_hej || kind == CHAT_2 || kind == LGF_2,
+                  "kernel %d with one unbounded direction is not supported by this library yet", kind);
+        E.k_cut = (kfact[E.ax[0]] + kfact[E.ax[1]] + kfact[E.ax[2]]) * 0.2;
+        E.hgrid = hfact[E.ax[0]] + hfact[E.ax[1]] + hfact[E.ax[2]];
+    } else {
+        E.hgrid = h[0];
+        E.set_g0 = (koffset[0] + koffset[1] + koffset[2] < 0.2);
+    }
+    if (!table.empty() && !dry) {
+        check_cuda(cudaMalloc(&d_table, table.size() * sizeof(double)), "LGF table");
+        check_cuda(cudaMemcpy(d_table, table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice), "LGF table");
+        E.table = d_table;
+    }
+    if (!far.empty() && !dry) {
+        check_cuda(cudaMalloc(&d_far, far.size() * sizeof(FarTerm)), "far field");
+        check_cuda(cudaMemcpy(d_far, far.data(), far.size() * sizeof(FarTerm), cudaMemcpyHostToDevice), "far field");
+        E.far = d_far;
+        E.nfar = (int)far.size();
+        E.far_log = far_log;
+    }
+    E.out = gb[0];
+    if (!dry) check_cuda(launch_green_eval(E, stream), "Green evaluation");
+
+    // forward transforms of the Green's function (Solver.cpp:1058-1076), FP64
+    ArrState cur;
+    for (int d = 0; d < 3; ++d) cur.n[d] = size0[d];
+    cur.cplx = cplx0;
+    int cb = 0;
+    for (int ip = 0; ip < ndim; ++ip) {
+        const DirPlan& p = grn[ip];
+        if (spec[p.dim]) continue;
+        // a real-to-real transform of complex storage acts on the real part only (the reference's
+        // r2r plan with stride nf = 2, src/FFTW_plan_dim.cpp:323-331); the imaginary part is zero here
+        ArrState nxt = cur;
+        nxt.n[p.dim] = p.n_out;
+        nxt.cplx = cur.cplx || p.isr2c;
+        PassArgs A = base_pass(p.dim, cur, 1, 1);
+        LineStage S;
+        memset(&S, 0, sizeof(S));
+        LineSpec& sp = S.spec[0];
+        sp.kind = (p.type == MIXUNB) ? LK_DCT1 : (p.isr2c ? LK_R2C : LK_C2C);
+        sp.sign = -1;
+        sp.n_in = p.n_in[0];
+        sp.fi = sp.fo = 0;
+        sp.postpro = PP_NONE;
+        S.spec[1] = S.spec[2] = sp;
+        S.M = fft_length(sp.kind, sp.n_in);
+        factorize(S.M, S);
+        S.n_b = p.isr2c ? 2 * p.n_out : p.n_out;
+        S.fieldstart = 0;
+        S.n_o = p.n_out;
+        S.in_cplx = cur.cplx;
+        S.out_cplx = nxt.cplx;
+        S.n_store = S.n_o;
+        S.tw = nullptr;
+        A.st[0] = S;
+        set_strides_internal(A.in_str, A.in_cstr, cur);
+        set_strides_internal(A.out_str, A.out_cstr, nxt);
+        A.in = gb[cb];
+        A.out = gb[1 - cb];
+        fit_lines(A, sizeof(double));
+        run_pass(A, true, true, true, "green");
+        cb = 1 - cb;
+        cur = nxt;
+    }
+
+    // folded layout of the working-precision copy
+    for (int d = 0; d < 3; ++d) {
+        gfold_M[d] = 0;
+        gfold_n[d] = st[ndim].n[d];
+    }
+    for (int ip = 0; ip < ndim; ++ip) {
+        const DirPlan& p = fwd[ip];
+        if ((p.type == PERPER || p.type == UNBUNB) && !p.isr2c) {
+            gfold_M[p.dim] = p.n_in[0];
+            gfold_n[p.dim] = p.n_in[0] / 2 + 1;
+        }
+    }
+    for (int d = 0; d < 3; ++d)
+        FLB_CHECK(spec_n[d] == st[ndim].n[d], "Topo of Green has to be the same as Topo of field");
+    gstr[0] = 1;
+    gstr[1] = gfold_n[0];
+    gstr[2] = (int64_t)gfold_n[0] * gfold_n[1];
+    const bool f64 = (precision == 64);
+    const size_t gsz = (size_t)gfold_n[0] * gfold_n[1] * gfold_n[2];
+    if (dry) return;
+    if (green) cudaFree(green);
+    check_cuda(cudaMalloc(&green, gsz * (f64 ? 8 : 4)), "Green spectrum");
+
+    GreenFinalArgs F;
+    memset(&F, 0, sizeof(F));
+    F.spec = gb[cb];
+    F.spec_cplx = cur.cplx;
+    for (int d = 0; d < 3; ++d) {
+        F.spec_n[d] = cur.n[d];
+        F.fold_n[d] = gfold_n[d];
+        F.fold_str[d] = gstr[d];
+    }
+    F.volfact = volfact;
+    F.complete = (ndim == 3 && nspec == 1 && (is_hej || is_lgf || is_meh));
+    if (F.complete) {
+        for (int d = 0; d < 3; ++d)
+            if (spec[d]) F.spec_dim = d;
+    }
+    F.kind = kind;
+    for (int ip = 0; ip < 3; ++ip) F.kfact[grn[ip].dim] = grn[ip].kfact;
+    for (int d = 0; d < 3; ++d) {
+        F.koffset[d] = koffset[d];
+        F.symstart[d] = symstart[d];
+    }
+    const int axl = grn[ndim - 1].dim;
+    F.ax[0] = axl;
+    F.ax[1] = (axl + 1) % 3;
+    F.ax[2] = (axl + 2) % 3;
+    F.hgrid = h[0];
+    F.length = length;
+    F.reset0 = (F.complete || nunb == 0) && (koffset[0] + koffset[1] + koffset[2] < 0.2);
+    F.out = green;
+    F.out_f64 = f64;
+    check_cuda(launch_green_final(F, stream), "Green finalisation");
+    check_cuda(cudaStreamSynchronize(stream), "Green setup");
+    cudaFree(gb[0]);
+    cudaFree(gb[1]);
+    if (d_table) cudaFree(d_table);
+    if (d_far) cudaFree(d_far);
+}
+
+// ---------------------------------------------------------------- setup / solve
+void Solver::setup() {
+    FLB_CHECK(!is_setup, "setup was already called");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    FLB_CHECK(e == cudaSuccess && ndev > 0, "no CUDA device available (%s): this library has no CPU path",
+              cudaGetErrorString(e));
+    compute_green();
+    ensure_buffers(1);
+    is_setup = true;
+}
+
+void Solver::ensure_buffers(int nbatch) {
+    const bool f64 = (precision == 64);
+    const size_t es = f64 ? 8 : 4;
+    for (int b = 0; b < 2; ++b) {
+        size_t need = 0;
+        for (int k = 1; k < ndim; ++k) {
+            if ((k - 1) % 2 != b) continue;
+            need = std::max(need, (size_t)st[k].n[0] * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch);
+        }
+        if (need > buf_elems[b]) {
+            if (buf[b]) cudaFree(buf[b]);
+            buf[b] = nullptr;
+            check_cuda(cudaMalloc(&buf[b], need * es), "work buffer");
+            buf_elems[b] = need;
+        }
+    }
+    buf_batch = std::max(buf_batch, nbatch);
+}
+
+size_t Solver::device_bytes(int nbatch) const {
+    const size_t es = (precision == 64) ? 8 : 4;
+    size_t total = 0;
+    for (int b = 0; b < 2; ++b) {
+        size_t need = 0;
+        for (int k = 1; k < ndim; ++k) {
+            if ((k - 1) % 2 != b) continue;
+            need = std::max(need, (size_t)st[k].n[0] * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch);
+        }
+        total += need * es;
+    }
+    total += (size_t)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
+    return total;
+}
+
+static bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+void Solver::do_fft_forward(const double* user_in, int nbatch) {
+    const bool f64 = (precision == 64);
+    const int es = f64 ? 8 : 4;
+    for (int ip = 0; ip < ndim - 1; ++ip) {
+        const DirPlan& p = fwd[ip];
+        PassArgs A = base_pass(p.dim, st[ip], lda * nbatch, lda);
+        A.st[0] = stage_forward(p, ip, f64);
+        if (ip == 0) {
+            set_strides_user(A.in_str, A.in_cstr);
+            A.in = user_in;
+        } else {
+            set_strides_internal(A.in_str, A.in_cstr, st[ip]);
+            A.in = buf[(ip - 1) % 2];
+        }
+        set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
+        A.out = buf[ip % 2];
+        fit_lines(A, es);
+        static const char* fn[3] = {"fwd0", "fwd1", "fwd2"};
+        run_pass(A, f64, ip == 0 ? true : f64, f64, fn[ip]);
+    }
+}
+
+void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
+    const bool f64 = (precision == 64);
+    const int es = f64 ? 8 : 4;
+    const int ipl = ndim - 1;
+    {
+        // fused: forward ndim-1, multiply, backward ndim-1 (in place on state ndim-1)
+        const DirPlan& p = fwd[ipl];
+        const DirPlan& pb = (type == ROT) ? dif[ipl] : bwd[ipl];
+        const bool rot = (type == ROT);
+        PassArgs A = base_pass(p.dim, st[ipl], lda * nbatch, lda);
+        A.fused = 1;
+        A.comps_together = rot ? 1 : 0;
+        if (rot) A.ncomp = 3;
+        A.st[0] = stage_forward(p, ipl, f64);
+        A.st[1] = stage_backward(pb, p, ipl, f64);
+        A.mult = mult_spec(type);
+        set_strides_internal(A.in_str, A.in_cstr, st[ipl]);
+        set_strides_internal(A.out_str, A.out_cstr, st[ipl]);
+        A.in = buf[(ipl - 1) % 2];
+        A.out = buf[(ipl - 1) % 2];
+        fit_lines(A, es);
+        if (rot && nbatch > 1) {
+            const int64_t per = A.in_cstr * 3 * (st[ipl].cplx ? 2 : 1);
+            for (int b = 0; b < nbatch; ++b) {
+                PassArgs B = A;
+                B.in = (const char*)A.in + (size_t)b * per * es;
+                B.out = (char*)A.out + (size_t)b * per * es;
+                run_pass(B, f64, f64, f64, "fused");
+            }
+        } else {
+            run_pass(A, f64, f64, f64, "fused");
+        }
+    }
+    for (int ip = ndim - 2; ip >= 0; --ip) {
+        const DirPlan& p = (type == ROT) ? dif[ip] : bwd[ip];
+        PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda * nbatch, lda);
+        A.st[0] = stage_backward(p, fwd[ip], ip, f64);
+        set_strides_internal(A.in_str, A.in_cstr, st[ip + 1]);
+        A.in = buf[ip % 2];
+        if (ip == 0) {
+            set_strides_user(A.out_str, A.out_cstr);
+            A.out = user_out;
+        } else {
+            set_strides_internal(A.out_str, A.out_cstr, st[ip]);
+            A.out = buf[(ip - 1) % 2];
+        }
+        fit_lines(A, es);
+        static const char* bn[3] = {"bwd0", "bwd1", "bwd2"};
+        run_pass(A, f64, f64, ip == 0 ? true : f64, bn[ip]);
+    }
+}
+
+void Solver::solve(double* field, double* rhs, int type, int nbatch) {
+    FLB_CHECK(is_setup, "flups_setup must be called before flups_solve");
+    FLB_CHECK((type == ROT && lda == 3) || (type != ROT), "You need vectors when using the ROT solver");
+    FLB_CHECK(!(type == ROT && odiff == NOD), "If calling the ROT solver, you need to initialize it with orderDiff = SPE or orderDiff = FD2");
+    FLB_CHECK((type == ROT && (odiff == SPE || odiff == FD2 || odiff == FD4 || odiff == FD6)) || (type != ROT),
+              "The differenciation order asked does not exist ");
+    FLB_CHECK(field != nullptr, "field is NULL");
+    FLB_CHECK(rhs != nullptr, "rhs is NULL");
+    FLB_CHECK(nbatch >= 1, "nbatch must be >= 1");
+    ensure_buffers(nbatch);
+    const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
+    const bool dev_in = is_device_ptr(rhs), dev_out = is_device_ptr(field);
+    double* din = rhs;
+    double* dout = field;
+    if (!dev_in || !dev_out) {
+        if (stage_elems < user_elems) {
+            if (stage_in) cudaFree(stage_in);
+            check_cuda(cudaMalloc(&stage_in, user_elems * sizeof(double)), "staging buffer");
+            stage_elems = user_elems;
+        }
+    }
+    if (!dev_in) {
+        check_cuda(cudaMemcpyAsync(stage_in, rhs, user_elems * sizeof(double), cudaMemcpyHostToDevice, stream), "rhs upload");
+        din = stage_in;
+    }
+    if (!dev_out) dout = stage_in;
+    pass_idx = 0;
+    do_fft_forward(din, nbatch);
+    do_fft_backward_fused(dout, type, nbatch);
+    collect_timing();
+    if (!dev_out) {
+        check_cuda(cudaMemcpyAsync(field, dout, user_elems * sizeof(double), cudaMemcpyDeviceToHost, stream), "field download");
+    }
+    if (!async || !dev_out || !dev_in) check_cuda(cudaStreamSynchronize(stream), "solve");
+    else check_cuda(cudaGetLastError(), "solve");
+}
+
+// ---------------------------------------------------------------- host-only description
+static void json_plan(std::string& o, const DirPlan& p) {
+    char b[1024];
+    snprintf(b, sizeof(b),
+             "{\"dim\":%d,\"type\":%d,\"n_out\":%d,\"fieldstart\":%d,\"koffset\":%.17g,\"kfact\":%.17g,\"symstart\":%.17g,"
+             "\"normfact\":%.17g,\"volfact\":%.17g,\"isr2c\":%d,\"is_spectral\":%d,\"comp\":[",
+             p.dim, p.type, p.n_out, p.fieldstart, p.koffset, p.kfact, p.symstart, p.normfact, p.volfact, p.isr2c ? 1 : 0,
+             p.is_spectral ? 1 : 0);
+    o += b;
+    for (int c = 0; c < p.lda; ++c) {
+        snprintf(b, sizeof(b), "%s{\"n_in\":%d,\"fi\":%d,\"fo\":%d,\"postpro\":%d,\"imult\":%d,\"kind\":%d}", c ? "," : "",
+                 p.n_in[c], p.fstart_in[c], p.fstart_out[c], p.postpro[c], p.imult[c] ? 1 : 0, p.kind[c]);
+        o += b;
+    }
+    o += "]}";
+}
+
+std::string Solver::plan_json(int type, int nbatch) {
+    std::string o = "{";
+    char b[512];
+    snprintf(b, sizeof(b), "\"ndim\":%d,\"normfact\":%.17g,\"volfact\":%.17g,\"plans\":{", ndim, normfact, volfact);
+    o += b;
+    const char* names[4] = {"fwd", "bwd", "grn", "dif"};
+    DirPlan* sets[4] = {fwd, bwd, grn, dif};
+    for (int k = 0; k < (have_diff ? 4 : 3); ++k) {
+        o += (k ? ",\"" : "\"");
+        o += names[k];
+        o += "\":[";
+        for (int ip = 0; ip < 3; ++ip) {
+            if (ip) o += ",";
+            json_plan(o, sets[k][ip]);
+        }
+        o += "]";
+    }
+    o += "},\"states\":[";
+    for (int k = 0; k <= ndim; ++k) {
+        snprintf(b, sizeof(b), "%s[%d,%d,%d,%d]", k ? "," : "", st[k].n[0], st[k].n[1], st[k].n[2], st[k].cplx ? 1 : 0);
+        o += b;
+    }
+    o += "],\"passes\":[";
+    dry = true;
+    dry_passes.clear();
+    dry_flags.clear();
+    dry_names.clear();
+    compute_green();
+    do_fft_forward(nullptr, nbatch);
+    do_fft_backward_fused(nullptr, type, nbatch);
+    dry = false;
+    for (size_t i = 0; i < dry_passes.size(); ++i) {
+        const PassArgs& A = dry_passes[i];
+        const int es = (dry_flags[i] & 1) ? 8 : 4;
+        snprintf(b, sizeof(b),
+                 "%s{\"name\":\"%s\",\"axis\":%d,\"n_src\":%d,\"n_a\":%d,\"n_b\":%d,\"ncomp\":%d,\"lda\":%d,\"lines_per_cta\":%d,"
+                 "\"fused\":%d,\"comps_together\":%d,\"flags\":%d,\"smem\":%zu,\"st\":[",
+                 i ? "," : "", dry_names[i].c_str(), A.axis, A.n_src, A.n_a, A.n_b, A.ncomp, A.lda, A.lines_per_cta, A.fused,
+                 A.comps_together, dry_flags[i], line_pass_smem(A, es));
+        o += b;
+        for (int s2 = 0; s2 <= A.fused; ++s2) {
+            const LineStage& S = A.st[s2];
+            snprintf(b, sizeof(b),
+                     "%s{\"M\":%d,\"nrad\":%d,\"n_b\":%d,\"fieldstart\":%d,\"n_o\":%d,\"in_cplx\":%d,\"out_cplx\":%d,"
+                     "\"store_off\":%d,\"n_store\":%d,\"spec\":[",
+                     s2 ? "," : "", S.M, S.nrad, S.n_b, S.fieldstart, S.n_o, S.in_cplx, S.out_cplx, S.store_off, S.n_store);
+            o += b;
+            for (int c = 0; c < lda; ++c) {
+                const LineSpec& sp = S.spec[c];
+                snprintf(b, sizeof(b), "%s{\"kind\":%d,\"sign\":%d,\"n_in\":%d,\"fi\":%d,\"fo\":%d,\"postpro\":%d,\"nfftw\":%d}",
+                         c ? "," : "", sp.kind, sp.sign, sp.n_in, sp.fi, sp.fo, sp.postpro, sp.nfftw);
+                o += b;
+            }
+            o += "]}";
+        }
+        o += "]}";
+    }
+    o += "]}";
+    return o;
+}

@@ -1,0 +1,314 @@
+"""Python front-end of libflups_b200.so, mirroring the reference's object
+interface (python_api/pyflups/flups.py: Topology, Profiler, Solver with
+set_green_type / set_alpha / setup / solve / get_alloc_size /
+get_spectral_info) over the same C symbols.
+
+Differences: no mpi4py (one rank; ``comm`` is ignored), arrays may be numpy
+arrays (host) or CUDA torch tensors (device pointers are passed through), and
+the added calls set_precision / solve_batch / device_bytes map to
+include/flups_b200.h.  The library must be built (``python -m
+flups_b200.build``); importing without it raises.
+"""
+import ctypes
+from ctypes import POINTER, c_bool, c_double, c_int, c_size_t, c_void_p
+from enum import IntEnum
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "libflups_b200.so"
+
+
+class BoundaryType(IntEnum):
+    EVEN = 0
+    ODD = 1
+    PER = 3
+    UNB = 4
+    NONE = 9
+
+
+class GreenType(IntEnum):
+    CHAT_2 = 0
+    LGF_2 = 1
+    HEJ_2 = 2
+    HEJ_4 = 3
+    HEJ_6 = 4
+    HEJ_8 = 5
+    HEJ_10 = 6
+    HEJ_0 = 7
+    LGF_4 = 8
+    LGF_6 = 9
+    LGF_8 = 10
+    MEHR_4L = 11
+    MEHR_6L = 12
+    MEHR_4F = 13
+    MEHR_6F = 14
+
+
+class SolverType(IntEnum):
+    STD = 0
+    ROT = 1
+
+
+class DiffType(IntEnum):
+    NOD = 0
+    SPE = 1
+    FD2 = 2
+    FD4 = 4
+    FD6 = 6
+
+
+class CenterType(IntEnum):
+    NODE_CENTER = 0
+    CELL_CENTER = 1
+
+
+FLUPS_FORWARD, FLUPS_BACKWARD, FLUPS_BACKWARD_DIFF, FLUPS_ALIGNMENT = -1, 1, 2, 8
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libflups_b200.so and declare the C signatures; raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else _LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m flups_b200.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(str(p))
+    vp, ip, dp = c_void_p, POINTER(c_int), POINTER(c_double)
+    sig = {
+        "flups_malloc": (vp, [c_size_t]),
+        "flups_free": (None, [vp]),
+        "flups_topo_new": (vp, [c_int, c_int, ip, ip, c_bool, ip, c_int, ctypes.c_ssize_t]),
+        "flups_topo_free": (None, [vp]),
+        "flups_topo_get_isComplex": (c_bool, [vp]),
+        "flups_topo_get_lda": (c_int, [vp]),
+        "flups_topo_get_axis": (c_int, [vp]),
+        "flups_topo_get_nglob": (c_int, [vp, c_int]),
+        "flups_topo_get_nloc": (c_int, [vp, c_int]),
+        "flups_topo_get_nmem": (c_int, [vp, c_int]),
+        "flups_topo_get_nproc": (c_int, [vp, c_int]),
+        "flups_topo_get_istartGlob": (None, [vp, ip]),
+        "flups_topo_get_locsize": (c_size_t, [vp]),
+        "flups_topo_get_memsize": (c_size_t, [vp]),
+        "flups_topo_cmpt_rank_fromid": (c_int, [vp, c_int, c_int]),
+        "flups_topo_cmpt_start_id_from_rank": (c_int, [vp, c_int, c_int]),
+        "flups_init": (vp, [vp, POINTER(POINTER(c_int)), dp, dp, c_int, ip]),
+        "flups_init_timed": (vp, [vp, POINTER(POINTER(c_int)), dp, dp, c_int, ip, vp]),
+        "flups_cleanup_solver": (None, [vp]),
+        "flups_cleanup_backend": (None, []),
+        "flups_set_greenType": (None, [vp, c_int]),
+        "flups_set_alpha": (None, [vp, c_double]),
+        "flups_set_stream": (None, [vp, vp]),
+        "flups_setup": (None, [vp, c_bool]),
+        "flups_solve": (None, [vp, vp, vp, c_int]),
+        "flups_solve_batch": (None, [vp, vp, vp, c_int, c_int]),
+        "flups_get_allocSize": (c_size_t, [vp]),
+        "flups_get_spectralInfo": (None, [vp, dp, dp, dp]),
+        "flups_pencilDirs": (None, [POINTER(POINTER(c_int)), ip]),
+        "flups_set_precision": (None, [vp, c_int]),
+        "flups_get_precision": (c_int, [vp]),
+        "flups_set_async": (None, [vp, c_int]),
+        "flups_get_last_error": (c_int, [vp]),
+        "flups_get_device_bytes": (c_size_t, [vp, c_int]),
+        "flups_b200_plan_json": (c_int, [vp, c_int, c_int, ctypes.c_char_p, c_int]),
+        "flups_set_pass_timing": (None, [vp, c_int]),
+        "flups_get_pass_stats": (c_int, [vp, c_int, dp, dp, POINTER(ctypes.c_long), ctypes.c_char_p, c_int]),
+        "flups_profiler_new_n": (vp, [ctypes.c_char_p]),
+        "flups_profiler_free": (None, [vp]),
+        "flups_profiler_disp": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    """Raw address of a numpy array or a torch tensor (host or device)."""
+    if hasattr(a, "data_ptr"):
+        return c_void_p(a.data_ptr())
+    return c_void_p(a.ctypes.data)
+
+
+class Topology:
+    """src/flups.h:210-349 (pyflups Topology)."""
+
+    def __init__(self, axis, lda, nglob, nproc=(1, 1, 1), is_complex=False, axproc=None, alignment=FLUPS_ALIGNMENT,
+                 comm=None):
+        lib = load_library()
+        ng = (c_int * 3)(*nglob)
+        npr = (c_int * 3)(*nproc)
+        axp = (c_int * 3)(*axproc) if axproc is not None else None
+        self._topo = lib.flups_topo_new(axis, lda, ng, npr, bool(is_complex), axp, alignment, 0)
+
+    def __del__(self):
+        if getattr(self, "_topo", None) and _lib is not None:
+            _lib.flups_topo_free(self._topo)
+            self._topo = None
+
+    @property
+    def _ptr(self):
+        return self._topo
+
+    @property
+    def lda(self):
+        return _lib.flups_topo_get_lda(self._topo)
+
+    @property
+    def axis(self):
+        return _lib.flups_topo_get_axis(self._topo)
+
+    def is_complex(self):
+        return bool(_lib.flups_topo_get_isComplex(self._topo))
+
+    def get_nglob(self, dim):
+        return _lib.flups_topo_get_nglob(self._topo, dim)
+
+    def get_nloc(self, dim):
+        return _lib.flups_topo_get_nloc(self._topo, dim)
+
+    def get_nmem(self, dim):
+        return _lib.flups_topo_get_nmem(self._topo, dim)
+
+    def get_nproc(self, dim):
+        return _lib.flups_topo_get_nproc(self._topo, dim)
+
+    def get_istart(self):
+        a = (c_int * 3)()
+        _lib.flups_topo_get_istartGlob(self._topo, a)
+        return np.array(a[:])
+
+    def locsize(self):
+        return _lib.flups_topo_get_locsize(self._topo)
+
+    def memsize(self):
+        return _lib.flups_topo_get_memsize(self._topo)
+
+
+class Profiler:
+    def __init__(self, name="default"):
+        self._prof = load_library().flups_profiler_new_n(name.encode())
+
+    def __del__(self):
+        if getattr(self, "_prof", None) and _lib is not None:
+            _lib.flups_profiler_free(self._prof)
+            self._prof = None
+
+    def display(self):
+        _lib.flups_profiler_disp(self._prof)
+
+    @property
+    def _ptr(self):
+        return self._prof
+
+
+class Solver:
+    """src/flups.h:369-578 (pyflups Solver).
+
+    ``boundary_conditions[d][side]`` is one BoundaryType, or a list with one
+    BoundaryType per component.
+    """
+
+    def __init__(self, topology, boundary_conditions, h, L, order_diff=DiffType.NOD, center_type=None, profiler=None):
+        lib = load_library()
+        self._topology = topology
+        lda = topology.lda
+        self._bc_arrays = []
+        for d in range(3):
+            for s in range(2):
+                v = boundary_conditions[d][s]
+                vals = list(v) if isinstance(v, (list, tuple)) else [v] * lda
+                self._bc_arrays.append((c_int * lda)(*[int(x) for x in vals]))
+        self._bc = (POINTER(c_int) * 6)(*[ctypes.cast(a, POINTER(c_int)) for a in self._bc_arrays])
+        hh = (c_double * 3)(*h)
+        LL = (c_double * 3)(*L)
+        ct = (c_int * 3)(*[int(c) for c in (center_type or [CenterType.CELL_CENTER] * 3)])
+        if profiler is None:
+            self._solver = lib.flups_init(topology._ptr, self._bc, hh, LL, int(order_diff), ct)
+        else:
+            self._solver = lib.flups_init_timed(topology._ptr, self._bc, hh, LL, int(order_diff), ct, profiler._ptr)
+
+    def __del__(self):
+        if getattr(self, "_solver", None) and _lib is not None:
+            _lib.flups_cleanup_solver(self._solver)
+            self._solver = None
+
+    def set_green_type(self, green_type):
+        _lib.flups_set_greenType(self._solver, int(green_type))
+
+    def set_alpha(self, alpha):
+        _lib.flups_set_alpha(self._solver, float(alpha))
+
+    def set_precision(self, bits):
+        _lib.flups_set_precision(self._solver, int(bits))
+
+    def set_stream(self, stream):
+        """stream: a torch.cuda.Stream or a raw cudaStream_t address."""
+        raw = getattr(stream, "cuda_stream", stream)
+        _lib.flups_set_stream(self._solver, c_void_p(raw))
+
+    def set_async(self, flag):
+        _lib.flups_set_async(self._solver, int(bool(flag)))
+
+    def setup(self, change_comm=False):
+        _lib.flups_setup(self._solver, bool(change_comm))
+
+    def solve(self, field, rhs, solver_type=SolverType.STD):
+        _lib.flups_solve(self._solver, _ptr(field), _ptr(rhs), int(solver_type))
+        return field
+
+    def solve_batch(self, field, rhs, nbatch, solver_type=SolverType.STD):
+        _lib.flups_solve_batch(self._solver, _ptr(field), _ptr(rhs), int(nbatch), int(solver_type))
+        return field
+
+    def get_alloc_size(self):
+        return _lib.flups_get_allocSize(self._solver)
+
+    def device_bytes(self, nbatch=1):
+        return _lib.flups_get_device_bytes(self._solver, int(nbatch))
+
+    def last_error(self):
+        return _lib.flups_get_last_error(self._solver)
+
+    def plan_json(self, solver_type=SolverType.STD, nbatch=1):
+        """Host-only description of the per-direction tables and the passes of one solve (no GPU needed)."""
+        import json
+        n = _lib.flups_b200_plan_json(self._solver, int(solver_type), int(nbatch), None, 0)
+        buf = ctypes.create_string_buffer(n)
+        _lib.flups_b200_plan_json(self._solver, int(solver_type), int(nbatch), buf, n)
+        return json.loads(buf.value.decode())
+
+    def set_pass_timing(self, on):
+        _lib.flups_set_pass_timing(self._solver, int(bool(on)))
+
+    def pass_stats(self):
+        """Per pass of one solve: name, accumulated ms, algorithmic bytes per launch, timed launches."""
+        n = _lib.flups_get_pass_stats(self._solver, 0, None, None, None, None, 0)
+        ms, by, ca = (c_double * n)(), (c_double * n)(), (ctypes.c_long * n)()
+        names = ctypes.create_string_buffer(32 * n)
+        _lib.flups_get_pass_stats(self._solver, n, ms, by, ca, names, 32)
+        out = []
+        for k in range(n):
+            nm = names.raw[32 * k:32 * (k + 1)].split(b"\0")[0].decode()
+            out.append({"name": nm, "ms_total": ms[k], "bytes": by[k], "calls": ca[k]})
+        return out
+
+    def get_spectral_info(self):
+        kf, ko, ss = (c_double * 3)(), (c_double * 3)(), (c_double * 3)()
+        _lib.flups_get_spectralInfo(self._solver, kf, ko, ss)
+        return np.array(kf[:]), np.array(ko[:]), np.array(ss[:])
+
+
+def pencil_dirs(boundary_conditions):
+    """flups_pencilDirs (src/flups.h:570)."""
+    lib = load_library()
+    arrs = [(c_int * 1)(int(boundary_conditions[d][s])) for d in range(3) for s in range(2)]
+    bc = (POINTER(c_int) * 6)(*[ctypes.cast(a, POINTER(c_int)) for a in arrs])
+    dirs = (c_int * 3)()
+    lib.flups_pencilDirs(bc, dirs)
+    return list(dirs)

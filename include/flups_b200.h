@@ -1,0 +1,75 @@
+/*
+ * flups_b200.h -- entry points added by the B200 library.  None changes the
+ * meaning of a reference call: a caller that never uses them gets the
+ * reference's behaviour (FP64 arithmetic, synchronous flups_solve).
+ */
+#ifndef FLUPS_B200_H
+#define FLUPS_B200_H
+
+#include <stddef.h>
+
+#include "flups_mpi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#else
+#include <stdbool.h>
+#endif
+
+struct Solver;
+struct Topology;
+
+/* Arithmetic of the per-solve transforms: 64 (default, as the reference) or
+ * 32 (FP32 transforms with FP64-computed twiddles and an FP32 copy of the
+ * FP64 Green's spectrum).  Must be called before flups_setup.  No reference
+ * counterpart (the reference is FP64 only, src/Solver.hpp:67,102). */
+void flups_set_precision(struct Solver* s, int bits);
+int flups_get_precision(struct Solver* s);
+
+/* Solve nbatch independent right-hand sides sharing one Green's spectrum in
+ * one sequence of launches.  rhs and field hold nbatch consecutive arrays of
+ * flups_topo_get_memsize(topo) doubles each (host or device pointers).  No
+ * reference counterpart; equivalent to nbatch calls of flups_solve. */
+void flups_solve_batch(struct Solver* s, double* field, double* rhs, int nbatch, int type);
+
+/* When set, flups_solve with device pointers returns without synchronising
+ * the solver's stream (host pointers always synchronise).  Default 0. */
+void flups_set_async(struct Solver* s, int async);
+
+/* Last CUDA error seen by the solver (0 = none).  No reference counterpart:
+ * the reference aborts on every error (src/defines.hpp:301-304). */
+int flups_get_last_error(struct Solver* s);
+
+/* Device bytes the solver holds after flups_setup (work buffers, Green's
+ * spectrum, twiddle tables) for nbatch right-hand sides. */
+size_t flups_get_device_bytes(struct Solver* s, int nbatch);
+
+/* Per-pass device timing of the following solves (CUDA events around each
+ * line pass on the solver's stream), for profiling; on = 0 stops recording
+ * and both calls reset the counters.  flups_get_pass_stats returns the number
+ * of passes per solve and fills, per pass, the accumulated milliseconds, the
+ * algorithmic bytes of one launch (source and kept output read/written once,
+ * the folded Green's spectrum once), the number of timed launches and a name
+ * (name_len bytes each).  Plays the part of the reference's profiler labels
+ * "fftw"/"SwitchTopo"/"domagic" (src/Solver.cpp:1411-1475). */
+void flups_set_pass_timing(struct Solver* s, int on);
+int flups_get_pass_stats(struct Solver* s, int maxn, double* ms_total, double* bytes, long* calls, char* names, int name_len);
+
+/* Host-only description (JSON) of the solver's per-direction tables and of
+ * the line passes one solve of kind type over nbatch right-hand sides would
+ * launch; needs no GPU.  Returns the length needed including the final NUL
+ * (the output is truncated to len).  For tests and tooling. */
+int flups_b200_plan_json(struct Solver* s, int type, int nbatch, char* out, int len);
+
+/* Alternative names of two reference calls:
+ * flups_init_topology == flups_topo_new (src/flups.h:210) and
+ * flups_solve_rot == flups_solve(..., ROT) (src/flups.h:452). */
+struct Topology* flups_init_topology(const int axis, const int lda, const int nglob[3], const int nproc[3], const bool isComplex,
+                                     const int axproc[3], const int alignment, MPI_Comm comm);
+void flups_solve_rot(struct Solver* s, double* field, double* rhs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -46,8 +46,16 @@ def farfield(name, n1, n2, n3=None):
     n3 = np.zeros_like(n1) if n3 is None else np.asarray(n3, dtype=np.float64)
     n = np.sqrt(n1 * n1 + n2 * n2 + n3 * n3)
     out = np.zeros(n.shape)
+    cache = {}
+
+    def pw(key, base, e):
+        k = (key, e)
+        if k not in cache:
+            cache[k] = base ** e if e != 0 else 1.0
+        return cache[k]
+
     for c, a, b, d, e, p in ent["terms"]:
-        out += c * n1 ** a * n2 ** b * n3 ** d * n ** e * math.pi ** p
+        out += (c * math.pi ** p) * pw(1, n1, a) * pw(2, n2, b) * pw(3, n3, d) * pw(0, n, e)
     for c, a, b, d, e, p in ent["log_terms"]:
         out += c * np.log(n)
     return out

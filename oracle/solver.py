@@ -197,13 +197,17 @@ class OracleSolver:
         A = [np.abs(I[ax[0]]), np.abs(I[ax[1]]), np.abs(I[ax[2]])]
         g = np.zeros(size)
         if nunb == 3:
-            r = np.sqrt(X[0] ** 2 + X[1] ** 2 + X[2] ** 2)
-            res = gk.green_3unb(kind, r, A[0], A[1], A[2], hfact[ax[0]], length, hfact[0] * hfact[1] * hfact[2])
-            if isinstance(res, tuple):
-                g, g0 = res
+            # only |is| matters here: evaluate on the distinct values per direction, then expand
+            uniq = [np.unique(np.abs(idx[d]), return_inverse=True) for d in range(3)]
+            U = np.meshgrid(uniq[0][0], uniq[1][0], uniq[2][0], indexing="ij")
+            UX = [U[d] * hfact[d] for d in range(3)]
+            UA = [U[ax[0]], U[ax[1]], U[ax[2]]]
+            r = np.sqrt(UX[0] ** 2 + UX[1] ** 2 + UX[2] ** 2)
+            res = gk.green_3unb(kind, r, UA[0], UA[1], UA[2], hfact[ax[0]], length, hfact[0] * hfact[1] * hfact[2])
+            gu, g0 = res if isinstance(res, tuple) else (res, None)
+            g = gu[np.ix_(uniq[0][1].ravel(), uniq[1][1].ravel(), uniq[2][1].ravel())]
+            if g0 is not None:
                 g[0, 0, 0] = g0
-            else:
-                g = res
         elif nunb == 2:
             r = np.sqrt(X[0] ** 2 + X[1] ** 2 + X[2] ** 2)
             k = K[0] + K[1] + K[2]
