@@ -233,6 +233,7 @@ void flups_set_precision(Solver* s, int bits) {
 }
 int flups_get_precision(Solver* s) { return s->precision; }
 void flups_set_async(Solver* s, int async) { s->async = async != 0; }
+void flups_b200_set_fast_kernels(Solver* s, int on) { s->use_fast = on != 0; }
 int flups_get_last_error(Solver* s) { return s->last_error; }
 size_t flups_get_device_bytes(Solver* s, int nbatch) { return s->device_bytes(nbatch); }
 

@@ -98,6 +98,61 @@ template <typename C> __device__ __forceinline__ void dft16(C* v) {
     for (int i = 0; i < 16; ++i) v[i] = t[i];
 }
 
+// W32^m = (cos(pi m/16), -sin(pi m/16)) for the m = n1*k2 products of dft32
+template <typename S> __device__ __forceinline__ void w32(int m, S& c, S& s) {
+    switch (m) {
+        case 0: c = (S)1; s = (S)0; break;
+        case 1: c = (S)0.98078528040323044913; s = -(S)0.19509032201612826785; break;
+        case 2: c = (S)0.92387953251128675613; s = -(S)0.38268343236508977173; break;
+        case 3: c = (S)0.83146961230254523708; s = -(S)0.55557023301960222474; break;
+        case 4: c = (S)0.70710678118654752440; s = -(S)0.70710678118654752440; break;
+        case 5: c = (S)0.55557023301960222474; s = -(S)0.83146961230254523708; break;
+        case 6: c = (S)0.38268343236508977173; s = -(S)0.92387953251128675613; break;
+        case 7: c = (S)0.19509032201612826785; s = -(S)0.98078528040323044913; break;
+        case 8: c = (S)0; s = (S)-1; break;
+        case 9: c = -(S)0.19509032201612826785; s = -(S)0.98078528040323044913; break;
+        case 10: c = -(S)0.38268343236508977173; s = -(S)0.92387953251128675613; break;
+        case 12: c = -(S)0.70710678118654752440; s = -(S)0.70710678118654752440; break;
+        case 14: c = -(S)0.92387953251128675613; s = -(S)0.38268343236508977173; break;
+        case 15: c = -(S)0.98078528040323044913; s = -(S)0.19509032201612826785; break;
+        case 18: c = -(S)0.92387953251128675613; s = (S)0.38268343236508977173; break;
+        case 21: c = -(S)0.55557023301960222474; s = (S)0.83146961230254523708; break;
+        default: c = (S)0; s = (S)0; break;
+    }
+}
+
+// DFT32 as 4 x 8: inner DFT8 over n2 of a[n1 + 4 n2], twiddle W32^{n1 k2}, outer DFT4 over n1
+template <typename C> __device__ __forceinline__ void dft32(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) {
+        C a[8];
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) a[n2] = v[n1 + 4 * n2];
+        dft8(a);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) v[n1 + 4 * k2] = a[k2];
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < 4; ++n1) {
+#pragma unroll
+        for (int k2 = 1; k2 < 8; ++k2) {
+            S c, s;
+            w32<S>(n1 * k2, c, s);
+            v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, s));
+        }
+    }
+    C t[32];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        C a0 = v[0 + 4 * k2], a1 = v[1 + 4 * k2], a2 = v[2 + 4 * k2], a3 = v[3 + 4 * k2];
+        dft4(a0, a1, a2, a3);
+        t[k2 + 0] = a0; t[k2 + 8] = a1; t[k2 + 16] = a2; t[k2 + 24] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = t[i];
+}
+
 template <typename C> __device__ __forceinline__ void dft3(C* v) {
     using S = decltype(v[0].x);
     const S h = (S)0.5, s3 = (S)0.86602540378443864676;

@@ -30,6 +30,10 @@ cudaError_t launch_line_pass(const PassArgs& A, int compute_f64, int in_f64, int
 size_t line_pass_smem(const PassArgs& A, int elem_bytes);
 cudaError_t launch_green_eval(const GreenEvalArgs& A, cudaStream_t s);
 cudaError_t launch_green_final(const GreenFinalArgs& A, cudaStream_t s);
+struct ColArgs;
+struct RowArgs;
+bool fast_col_supported(int L);
+bool fast_row_supported(int L);
 
 // plan types and FFTW r2r kinds (src/FFTW_plan_dim.hpp:34-62)
 enum PlanType { SYMSYM = 2, MIXUNB = 5, PERPER = 6, UNBUNB = 8, EMPTY = 18 };
@@ -137,6 +141,8 @@ struct Solver {
     std::vector<flb::PassArgs> dry_passes;
     std::vector<int> dry_flags;
     std::vector<std::string> dry_names;
+    std::vector<int> dry_fast;
+    bool use_fast = true;                 // register-resident power-of-two kernels where they apply
     // ---------------------------------------------------------------- per-pass timing
     bool timing = false;
     int pass_idx = 0;
@@ -158,6 +164,9 @@ struct Solver {
     void dry_run(flb::DirPlan p[3]);
     void compute_green();
     const void* twiddle(int M, bool f64);
+    const void* twiddle_plain(int L, bool f64);   // W_L^q, q < L
+    int fast_kind(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64) const;  // 0 none, 1 column, 2 row
+    void launch_fast(const flb::PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64);
     void ensure_buffers(int nbatch);
     flb::LineStage stage_forward(const flb::DirPlan& p, int ip, bool f64);
     flb::LineStage stage_backward(const flb::DirPlan& p, const flb::DirPlan& pf, int ip, bool f64);

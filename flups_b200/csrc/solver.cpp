@@ -22,6 +22,35 @@
 using namespace flb;
 
 namespace flb {
+struct ColArgs {
+    const void* in;
+    void* out;
+    int nx;
+    int nin, nout;
+    int64_t in_lstr, in_ostr, in_cstr;
+    int64_t out_lstr, out_ostr, out_cstr;
+    int nouter;
+    const void* tw;
+    const void* green;
+    int64_t g_x, g_line, g_outer;
+    int f_x, f_line, f_outer;
+    double normfact;
+};
+struct RowArgs {
+    const void* in;
+    void* out;
+    int nrows;
+    int n1;
+    int nin;
+    int nout;
+    int64_t in_s1, in_s2, in_cstr;
+    int64_t out_s1, out_s2, out_cstr;
+    int in_f64, out_f64;
+    const void* tw;
+    const void* twh;
+};
+cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 int load_lgf_table(int kind, int ndim, std::vector<double>& data);
 int farfield_terms(int kind, int ndim, std::vector<FarTerm>& terms, double& logc);
 }  // namespace flb
@@ -365,12 +394,140 @@ MultSpec Solver::mult_spec(int type) const {
     return G;
 }
 
+// Which register-resident kernel can run this pass (0 = none: the general line pass).
+int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) const {
+    if (!use_fast || A.comps_together) return 0;
+    const int nst = A.fused ? 2 : 1;
+    for (int s2 = 0; s2 < nst; ++s2) {
+        const LineStage& S = A.st[s2];
+        for (int c = 0; c < A.lda; ++c) {
+            const LineSpec& sp = S.spec[c];
+            if (sp.fi != 0 || sp.fo != 0 || sp.postpro != PP_NONE) return 0;
+            if (sp.kind != S.spec[0].kind || sp.n_in != S.spec[0].n_in) return 0;
+        }
+        if (S.fieldstart != 0 || S.store_off != 0) return 0;
+    }
+    const LineStage& S0 = A.st[0];
+    const int k0 = S0.spec[0].kind;
+    if (A.axis != 0) {
+        // columns: complex DFT, working precision in and out, x contiguous
+        if (k0 != LK_C2C || !S0.in_cplx || !S0.out_cplx || in_f64 != f64 || out_f64 != f64) return 0;
+        if (A.fused && (A.st[1].spec[0].kind != LK_C2C || A.st[1].M != S0.M || A.mult.mode != 1)) return 0;
+        if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
+        const int L = S0.M;
+        if (!fast_col_supported(L) || A.n_src > L) return 0;
+        const LineStage& SL = A.st[A.fused ? 1 : 0];
+        if (SL.n_store > L) return 0;
+        if (!A.fused && S0.n_o != L) return 0;
+        return 1;
+    }
+    if (A.fused) return 0;
+    const int L = S0.M;
+    if (!fast_row_supported(L) || A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
+    auto even = [](int64_t v) { return (v % 2) == 0; };
+    if (k0 == LK_R2C) {
+        if (S0.in_cplx || !S0.out_cplx || A.n_src > L || S0.n_o != L / 2 + 1 || S0.n_store != S0.n_o) return 0;
+        if (!even(A.in_str[1]) || !even(A.in_str[2]) || !even(A.in_cstr)) return 0;
+        if (out_f64 != f64) return 0;
+        return 2;
+    }
+    if (k0 == LK_C2R) {
+        if (!S0.in_cplx || S0.out_cplx || A.n_src != L / 2 + 1 || S0.n_store > L) return 0;
+        if (!even(A.out_str[1]) || !even(A.out_str[2]) || !even(A.out_cstr)) return 0;
+        if (in_f64 != f64) return 0;
+        return 2;
+    }
+    return 0;
+}
+
+void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64) {
+    const LineStage& S0 = A.st[0];
+    const int L = S0.M;
+    const int b = (A.axis == 2) ? 1 : 2;
+    if (kind == 1) {
+        ColArgs c;
+        memset(&c, 0, sizeof(c));
+        c.in = A.in;
+        c.out = A.out;
+        c.nx = A.n_a;
+        c.nouter = A.n_b;
+        c.nin = A.n_src;
+        c.nout = A.st[A.fused ? 1 : 0].n_store;
+        c.in_lstr = A.in_str[A.axis];
+        c.in_ostr = A.in_str[b];
+        c.in_cstr = A.in_cstr;
+        c.out_lstr = A.out_str[A.axis];
+        c.out_ostr = A.out_str[b];
+        c.out_cstr = A.out_cstr;
+        c.tw = twiddle_plain(L, f64);
+        int mode = (S0.spec[0].sign > 0) ? 1 : 0;
+        if (A.fused) {
+            mode = 2;
+            c.green = A.mult.green;
+            c.g_x = A.mult.gstr[0];
+            c.g_line = A.mult.gstr[A.axis];
+            c.g_outer = A.mult.gstr[b];
+            c.f_x = A.mult.gfold[0];
+            c.f_line = A.mult.gfold[A.axis];
+            c.f_outer = A.mult.gfold[b];
+            c.normfact = A.mult.normfact;
+        }
+        check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
+        return;
+    }
+    RowArgs r;
+    memset(&r, 0, sizeof(r));
+    r.in = A.in;
+    r.out = A.out;
+    r.n1 = A.n_a;
+    r.nrows = A.n_a * A.n_b;
+    r.nin = A.n_src;
+    r.nout = S0.n_store;
+    r.in_s1 = A.in_str[1];
+    r.in_s2 = A.in_str[2];
+    r.in_cstr = A.in_cstr;
+    r.out_s1 = A.out_str[1];
+    r.out_s2 = A.out_str[2];
+    r.out_cstr = A.out_cstr;
+    r.in_f64 = in_f64;
+    r.out_f64 = out_f64;
+    r.tw = twiddle_plain(L, f64);
+    r.twh = twiddle_plain(L / 2, f64);
+    check_cuda(launch_fast_row(f64, S0.spec[0].kind == LK_C2R, L, r, A.ncomp, stream), "row DFT launch");
+}
+
+const void* Solver::twiddle_plain(int L, bool f64) {
+    const int64_t key = -((int64_t)L * 2 + (f64 ? 1 : 0));
+    auto it = twiddles.find(key);
+    if (it != twiddles.end()) return it->second;
+    std::vector<double> w(2 * (size_t)L);
+    for (int q = 0; q < L; ++q) {
+        const long double a = -2.0L * (long double)M_PI * (long double)q / (long double)L;
+        w[2 * q] = (double)cosl(a);
+        w[2 * q + 1] = (double)sinl(a);
+    }
+    void* d = nullptr;
+    if (f64) {
+        check_cuda(cudaMalloc(&d, w.size() * sizeof(double)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice), "twiddle upload");
+    } else {
+        std::vector<float> wf(w.size());
+        for (size_t i = 0; i < w.size(); ++i) wf[i] = (float)w[i];
+        check_cuda(cudaMalloc(&d, wf.size() * sizeof(float)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice), "twiddle upload");
+    }
+    twiddles[key] = d;
+    return d;
+}
+
 void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, const char* name) {
     PassArgs A = Ain;
+    const int fk = fast_kind(A, f64, in_f64, out_f64);
     if (dry) {
         dry_passes.push_back(A);
         dry_flags.push_back((f64 ? 1 : 0) | (in_f64 ? 2 : 0) | (out_f64 ? 4 : 0));
         dry_names.push_back(name);
+        dry_fast.push_back(fk);
         return;
     }
     for (int s2 = 0; s2 <= A.fused; ++s2)
@@ -399,7 +556,8 @@ void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, 
         }
         cudaEventRecord(ev[2 * k], stream);
     }
-    check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
+    if (fk) launch_fast(A, fk, f64, in_f64, out_f64);
+    else check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
     if (timing) cudaEventRecord(ev[2 * k + 1], stream);
 }
 
@@ -869,6 +1027,7 @@ std::string Solver::plan_json(int type, int nbatch) {
     dry_passes.clear();
     dry_flags.clear();
     dry_names.clear();
+    dry_fast.clear();
     compute_green();
     do_fft_forward(nullptr, nbatch);
     do_fft_backward_fused(nullptr, type, nbatch);
@@ -878,9 +1037,9 @@ std::string Solver::plan_json(int type, int nbatch) {
         const int es = (dry_flags[i] & 1) ? 8 : 4;
         snprintf(b, sizeof(b),
                  "%s{\"name\":\"%s\",\"axis\":%d,\"n_src\":%d,\"n_a\":%d,\"n_b\":%d,\"ncomp\":%d,\"lda\":%d,\"lines_per_cta\":%d,"
-                 "\"fused\":%d,\"comps_together\":%d,\"flags\":%d,\"smem\":%zu,\"st\":[",
+                 "\"fused\":%d,\"comps_together\":%d,\"flags\":%d,\"fast\":%d,\"smem\":%zu,\"st\":[",
                  i ? "," : "", dry_names[i].c_str(), A.axis, A.n_src, A.n_a, A.n_b, A.ncomp, A.lda, A.lines_per_cta, A.fused,
-                 A.comps_together, dry_flags[i], line_pass_smem(A, es));
+                 A.comps_together, dry_flags[i], dry_fast[i], line_pass_smem(A, es));
         o += b;
         for (int s2 = 0; s2 <= A.fused; ++s2) {
             const LineStage& S = A.st[s2];

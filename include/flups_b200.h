@@ -61,6 +61,11 @@ int flups_get_pass_stats(struct Solver* s, int maxn, double* ms_total, double* b
  * (the output is truncated to len).  For tests and tooling. */
 int flups_b200_plan_json(struct Solver* s, int type, int nbatch, char* out, int len);
 
+/* Use (1, default) or bypass (0) the register-resident power-of-two DFT
+ * kernels; with 0 every pass runs through the general line-pass kernel.
+ * For cross-checking the two kernel families. */
+void flups_b200_set_fast_kernels(struct Solver* s, int on);
+
 /* Alternative names of two reference calls:
  * flups_init_topology == flups_topo_new (src/flups.h:210) and
  * flups_solve_rot == flups_solve(..., ROT) (src/flups.h:452). */
