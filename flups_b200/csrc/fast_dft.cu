@@ -328,14 +328,14 @@ static cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
 template <typename T, int MODE>
 static cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
-    constexpr int TX = sizeof(T) == 4 ? 8 : 4;
+    constexpr int TX = sizeof(T) == 4 ? 8 : 4;  // one 64-byte segment of a row per warp access
     switch (L) {
         case 64: return launch_col_t<T, 64, R1, TX, MODE>(a, ncomp, s);
         case 128: return launch_col_t<T, 128, R1, TX, MODE>(a, ncomp, s);
         case 256: return launch_col_t<T, 256, R1, TX, MODE>(a, ncomp, s);
         case 512: return launch_col_t<T, 512, R1, TX, MODE>(a, ncomp, s);
         case 1024: return launch_col_t<T, 1024, R1, TX, MODE>(a, ncomp, s);
-        case 2048: return launch_col_t<T, 2048, R1, TX, MODE>(a, ncomp, s);
+        case 2048: return launch_col_t<T, 2048, R1, TX / 2, MODE>(a, ncomp, s);  // keep CTAs at 256 threads
     }
     return cudaErrorInvalidValue;
 }

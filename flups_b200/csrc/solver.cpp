@@ -397,6 +397,10 @@ MultSpec Solver::mult_spec(int type) const {
 // Which register-resident kernel can run this pass (0 = none: the general line pass).
 int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) const {
     if (!use_fast || A.comps_together) return 0;
+    if (A.n_b > 65535 || A.ncomp > 65535) return 0;  // grid y / z limits of the fast launches
+    // vector loads/stores of complex (or real pairs) need their natural alignment
+    const uintptr_t ain = dry ? 0 : (uintptr_t)A.in, aout = dry ? 0 : (uintptr_t)A.out;
+    if ((ain % (in_f64 ? 16 : 8)) != 0 || (aout % (out_f64 ? 16 : 8)) != 0) return 0;
     const int nst = A.fused ? 2 : 1;
     for (int s2 = 0; s2 < nst; ++s2) {
         const LineStage& S = A.st[s2];

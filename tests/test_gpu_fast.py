@@ -1,0 +1,71 @@
+"""The register-resident power-of-two DFT kernels (flups_b200/csrc/fast_dft.cu)
+against the oracle and against the general line-pass kernel, on grids where
+they are selected (checked through the host-side plan description)."""
+import numpy as np
+import pytest
+
+from gpu_helpers import from_user, make_solver, oracle_solve, rel_l2, to_user
+from oracle.plans import CELL_CENTER, NODE_CENTER, CHAT_2, LGF_2, HEJ_2, HEJ_4
+
+pytestmark = pytest.mark.gpu
+
+UNB3 = [[[4], [4]]] * 3
+PPU = [[[3], [3]], [[3], [3]], [[4], [4]]]
+
+
+def _rhs(nglob, lda=1, seed=3):
+    rng = np.random.default_rng(seed)
+    x = [np.arange(n) / n for n in nglob]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    out = np.zeros((lda,) + tuple(nglob))
+    for c in range(lda):
+        for _ in range(4):
+            cc = rng.uniform(0.3, 0.7, 3)
+            s = rng.uniform(0.05, 0.1)
+            out[c] += rng.uniform(-1, 1) * np.exp(-((X - cc[0]) ** 2 + (Y - cc[1]) ** 2 + (Z - cc[2]) ** 2) / s ** 2)
+    return out
+
+
+def _run(nglob, lda, bcv, center, kernel, precision, fast):
+    n0 = nglob[0] - (0 if center == CELL_CENTER else 1)
+    h = [1.0 / n0] * 3
+    L = [h[d] * (nglob[d] - (0 if center == CELL_CENTER else 1)) for d in range(3)]
+    t, s = make_solver(nglob, lda, bcv, h, L, center, kernel, precision=precision)
+    from flups_b200 import pyflups as pf
+    pf.load_library().flups_b200_set_fast_kernels(s._solver, int(fast))
+    plan = s.plan_json()
+    rhs = _rhs(nglob, lda)
+    u = to_user(rhs)
+    out = np.zeros_like(u)
+    s.solve(out, u)
+    assert s.last_error() == 0
+    ref = oracle_solve(nglob, lda, bcv, h, L, center, kernel, rhs)
+    return from_user(out, lda, nglob), ref, plan
+
+
+CASES = [
+    ("unb64_chat2", [64] * 3, 1, UNB3, CELL_CENTER, CHAT_2),
+    ("unb32_hej2", [32] * 3, 1, UNB3, CELL_CENTER, HEJ_2),
+    ("unb128_lgf2", [128] * 3, 1, UNB3, CELL_CENTER, LGF_2),
+    ("unb_aniso", [128, 64, 32], 1, UNB3, CELL_CENTER, CHAT_2),
+    ("ppu64_hej4", [64] * 3, 1, PPU, CELL_CENTER, HEJ_4),
+    ("node65_unb", [65] * 3, 1, UNB3, NODE_CENTER, CHAT_2),
+    ("vector3_unb64", [64] * 3, 3, [[[4] * 3, [4] * 3]] * 3, CELL_CENTER, LGF_2),
+]
+
+
+@pytest.mark.parametrize("name,nglob,lda,bcv,center,kernel", CASES, ids=[c[0] for c in CASES])
+def test_fast_fp64_matches_oracle(name, nglob, lda, bcv, center, kernel):
+    got, ref, plan = _run(nglob, lda, bcv, center, kernel, 64, True)
+    assert any(p["fast"] for p in plan["passes"] if p["name"] != "green"), "fast kernels not selected"
+    assert rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("name,nglob,lda,bcv,center,kernel", CASES, ids=[c[0] for c in CASES])
+def test_fast_fp32_matches_oracle_and_general_engine(name, nglob, lda, bcv, center, kernel):
+    got, ref, _ = _run(nglob, lda, bcv, center, kernel, 32, True)
+    gen, _, plan = _run(nglob, lda, bcv, center, kernel, 32, False)
+    assert not any(p["fast"] for p in plan["passes"])
+    assert rel_l2(got, ref) <= 2e-6
+    assert rel_l2(gen, ref) <= 2e-6
+    assert rel_l2(got, gen) <= 2e-6
