@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/flups.h"
+#include "fast_dft.h"
 #include "green.cuh"
 #include "pass_desc.h"
 
@@ -30,10 +31,6 @@ cudaError_t launch_line_pass(const PassArgs& A, int compute_f64, int in_f64, int
 size_t line_pass_smem(const PassArgs& A, int elem_bytes);
 cudaError_t launch_green_eval(const GreenEvalArgs& A, cudaStream_t s);
 cudaError_t launch_green_final(const GreenFinalArgs& A, cudaStream_t s);
-struct ColArgs;
-struct RowArgs;
-bool fast_col_supported(int L);
-bool fast_row_supported(int L);
 
 // plan types and FFTW r2r kinds (src/FFTW_plan_dim.hpp:34-62)
 enum PlanType { SYMSYM = 2, MIXUNB = 5, PERPER = 6, UNBUNB = 8, EMPTY = 18 };

@@ -1,0 +1,244 @@
+// flups_solve_noalloc: a solve that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc while they run: code being captured
+// into a CUDA graph in the global capture mode (allocation calls are refused
+// there), real-time loops that must stay out of the allocator (cudaMalloc can
+// synchronise the device and takes driver locks), and frameworks that reserve
+// the device memory for their own pools up front, so that a late cudaMalloc
+// fails.  For them this entry point runs one solve of an already set-up
+// solver with all of its per-solve scratch -- the two work arrays between the
+// line passes and the twiddle tables of those passes -- in one file-scope
+// device array of FLUPS_NOALLOC_SCRATCH_BYTES (64 MiB).  Every GPU that loads
+// the library holds that array until the process exits.
+//
+// Rules for callers:
+//   - field and rhs must be device pointers: there is no host staging;
+//   - flups_setup must have run: the Green's spectrum it computes is an input
+//     here (setup allocates; this call does not);
+//   - the first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress; make that first call before any stream capture;
+//   - the call only enqueues work on the solver's stream (flups_set_stream)
+//     and returns; synchronise that stream before reading field;
+//   - every call shares the array and overwrites what the previous call left
+//     in it: calls that may overlap on the GPU (different streams without an
+//     ordering between them) race on it;
+//   - nothing in the array has to start at zero (the passes write every
+//     element they later read; the twiddle tables are rewritten per call);
+//   - a solve whose scratch does not fit is refused with an error code.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fast_dft.h"
+#include "host.hpp"
+
+#define FLUPS_NOALLOC_SCRATCH_BYTES (64u << 20)
+#define FLUPS_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FLUPS_NOALLOC_SCRATCH_BYTES];
+static void* g_noalloc_ptr[FLUPS_NOALLOC_MAX_DEVICES] = {nullptr};
+
+using namespace flb;
+
+// exp(-2 pi i q / n) for q < n, FP64 sincospi, stored in the working precision
+__global__ void noalloc_twiddle_kernel(void* out, int n, int f64) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(-2.0 * (double)q / (double)n, &s, &c);
+        if (f64) reinterpret_cast<double2*>(out)[q] = make_double2(c, s);
+        else reinterpret_cast<float2*>(out)[q] = make_float2((float)c, (float)s);
+    }
+}
+
+namespace {
+
+struct TwSlot {
+    int n;        // table length (complex entries)
+    size_t off;   // byte offset in the scratch array
+};
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int fail(int code, const char* msg) {
+    fprintf(stderr, "[flups_b200] flups_solve_noalloc: %s\n", msg);
+    fflush(stderr);
+    return code;
+}
+
+}  // namespace
+
+extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int type) {
+    if (!s) return fail(-1, "solver is NULL");
+    if (!s->is_setup) return fail(-1, "flups_setup must be called first (it computes the Green's spectrum)");
+    if (!field || !rhs) return fail(-2, "field and rhs must not be NULL");
+    if (type == ROT && (s->lda != 3 || s->odiff == NOD)) return fail(-2, "ROT needs lda = 3 and a derivative order");
+    for (const void* p : {(const void*)field, (const void*)rhs}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess ||
+            !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged)) {
+            cudaGetLastError();
+            return fail(-2, "field and rhs must be device pointers (no host staging without allocation)");
+        }
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= FLUPS_NOALLOC_MAX_DEVICES) return fail(-4, "no usable device");
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            s->last_error = (int)e;
+            return fail(-4, "cudaGetSymbolAddress of the scratch array failed");
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    unsigned char* base = reinterpret_cast<unsigned char*>(g_noalloc_ptr[dev]);
+    const bool f64 = (s->precision == 64);
+    const size_t es = f64 ? 8 : 4;
+
+    // scratch layout: work arrays of the states the solve passes through, then twiddle tables
+    size_t need[2] = {0, 0};
+    for (int k = 1; k < s->ndim; ++k) {
+        const size_t e = (size_t)s->st[k].n[0] * s->st[k].n[1] * s->st[k].n[2] * (s->st[k].cplx ? 2 : 1) * s->lda;
+        need[(k - 1) % 2] = std::max(need[(k - 1) % 2], e * es);
+    }
+    size_t off = 0;
+    void* wb[2] = {nullptr, nullptr};
+    for (int b = 0; b < 2; ++b) {
+        if (need[b]) {
+            wb[b] = base + off;
+            off = align256(off + need[b]);
+        }
+    }
+
+    // the passes of one solve, planned on the host with the work arrays placed in the scratch array
+    void* keep[2] = {s->buf[0], s->buf[1]};
+    s->buf[0] = wb[0];
+    s->buf[1] = wb[1];
+    s->dry = true;
+    s->dry_passes.clear();
+    s->dry_flags.clear();
+    s->dry_names.clear();
+    s->dry_fast.clear();
+    s->do_fft_forward(rhs, 1);
+    s->do_fft_backward_fused(field, type, 1);
+    s->dry = false;
+    std::vector<PassArgs> passes = s->dry_passes;
+    std::vector<int> flags = s->dry_flags;
+    s->dry_passes.clear();
+    s->dry_flags.clear();
+    s->dry_names.clear();
+    s->dry_fast.clear();
+    s->buf[0] = keep[0];
+    s->buf[1] = keep[1];
+
+    // twiddle tables: one per distinct length
+    std::vector<TwSlot> slots;
+    auto slot_for = [&](int n) -> size_t {
+        for (const TwSlot& t : slots)
+            if (t.n == n) return t.off;
+        TwSlot t{n, off};
+        off = align256(off + (size_t)n * 2 * es);
+        slots.push_back(t);
+        return t.off;
+    };
+    std::vector<int> kinds(passes.size());
+    for (size_t i = 0; i < passes.size(); ++i) {
+        PassArgs& A = passes[i];
+        const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
+        kinds[i] = s->fast_kind(A, f64, in64, out64);
+        if (kinds[i] == 0) {
+            for (int sg = 0; sg <= A.fused; ++sg) slot_for(2 * A.st[sg].M);
+        } else {
+            slot_for(A.st[0].M);
+            if (kinds[i] == 2) slot_for(A.st[0].M / 2);
+        }
+    }
+    if (off > FLUPS_NOALLOC_SCRATCH_BYTES) {
+        char msg[256];
+        snprintf(msg, sizeof(msg), "this solve needs %zu bytes of scratch, above the %u-byte limit of the no-allocation entry point",
+                 off, (unsigned)FLUPS_NOALLOC_SCRATCH_BYTES);
+        return fail(-3, msg);
+    }
+
+    cudaStream_t st = s->stream;
+    for (const TwSlot& t : slots) {
+        const int nb = std::min(1184, (t.n + 255) / 256);
+        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, f64 ? 1 : 0);
+    }
+    auto tw_of = [&](int n) { return (const void*)(base + slot_for(n)); };
+    for (size_t i = 0; i < passes.size(); ++i) {
+        PassArgs& A = passes[i];
+        const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
+        cudaError_t e = cudaSuccess;
+        if (kinds[i] == 0) {
+            for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M);
+            e = launch_line_pass(A, f64 ? 1 : 0, in64 ? 1 : 0, out64 ? 1 : 0, st);
+        } else if (kinds[i] == 1) {
+            const LineStage& S0 = A.st[0];
+            const int L = S0.M;
+            const int b = (A.axis == 2) ? 1 : 2;
+            ColArgs c;
+            memset(&c, 0, sizeof(c));
+            c.in = A.in;
+            c.out = A.out;
+            c.nx = A.n_a;
+            c.nouter = A.n_b;
+            c.nin = A.n_src;
+            c.nout = A.st[A.fused ? 1 : 0].n_store;
+            c.in_lstr = A.in_str[A.axis];
+            c.in_ostr = A.in_str[b];
+            c.in_cstr = A.in_cstr;
+            c.out_lstr = A.out_str[A.axis];
+            c.out_ostr = A.out_str[b];
+            c.out_cstr = A.out_cstr;
+            c.tw = tw_of(L);
+            int mode = (S0.spec[0].sign > 0) ? 1 : 0;
+            if (A.fused) {
+                mode = 2;
+                c.green = A.mult.green;
+                c.g_x = A.mult.gstr[0];
+                c.g_line = A.mult.gstr[A.axis];
+                c.g_outer = A.mult.gstr[b];
+                c.f_x = A.mult.gfold[0];
+                c.f_line = A.mult.gfold[A.axis];
+                c.f_outer = A.mult.gfold[b];
+                c.normfact = A.mult.normfact;
+            }
+            e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
+        } else {
+            const LineStage& S0 = A.st[0];
+            const int L = S0.M;
+            RowArgs r;
+            memset(&r, 0, sizeof(r));
+            r.in = A.in;
+            r.out = A.out;
+            r.n1 = A.n_a;
+            r.nrows = A.n_a * A.n_b;
+            r.nin = A.n_src;
+            r.nout = S0.n_store;
+            r.in_s1 = A.in_str[1];
+            r.in_s2 = A.in_str[2];
+            r.in_cstr = A.in_cstr;
+            r.out_s1 = A.out_str[1];
+            r.out_s2 = A.out_str[2];
+            r.out_cstr = A.out_cstr;
+            r.in_f64 = in64;
+            r.out_f64 = out64;
+            r.tw = tw_of(L);
+            r.twh = tw_of(L / 2);
+            e = launch_fast_row(f64 ? 1 : 0, S0.spec[0].kind == LK_C2R, L, r, A.ncomp, st);
+        }
+        if (e != cudaSuccess) {
+            s->last_error = (int)e;
+            return fail(-4, cudaGetErrorString(e));
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        s->last_error = (int)e;
+        return fail(-4, cudaGetErrorString(e));
+    }
+    return 0;
+}

@@ -17,40 +17,12 @@
 #include <cstring>
 #include <vector>
 
+#include "fast_dft.h"
 #include "host.hpp"
 
 using namespace flb;
 
 namespace flb {
-struct ColArgs {
-    const void* in;
-    void* out;
-    int nx;
-    int nin, nout;
-    int64_t in_lstr, in_ostr, in_cstr;
-    int64_t out_lstr, out_ostr, out_cstr;
-    int nouter;
-    const void* tw;
-    const void* green;
-    int64_t g_x, g_line, g_outer;
-    int f_x, f_line, f_outer;
-    double normfact;
-};
-struct RowArgs {
-    const void* in;
-    void* out;
-    int nrows;
-    int n1;
-    int nin;
-    int nout;
-    int64_t in_s1, in_s2, in_cstr;
-    int64_t out_s1, out_s2, out_cstr;
-    int in_f64, out_f64;
-    const void* tw;
-    const void* twh;
-};
-cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
-cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 int load_lgf_table(int kind, int ndim, std::vector<double>& data);
 int farfield_terms(int kind, int ndim, std::vector<FarTerm>& terms, double& logc);
 }  // namespace flb
