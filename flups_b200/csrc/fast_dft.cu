@@ -32,12 +32,17 @@ __device__ __forceinline__ void dftr(C* v) {
     else if constexpr (R == 32) dft32(v);
 }
 
-template <typename T, int L, int R1>
+// ROWS: the lines of a CTA are thread-index-slow (row passes: p fastest),
+// else thread-index-fast (column passes: the TX columns fastest).
+template <typename T, int L, int R1, bool ROWS = false>
 struct RegFFT {
     using C = typename CT<T>::C;
     static constexpr int P = L / R1;
-    // line stride in shared memory: swizzled length rounded to 16 plus 2 (bank spread across lines)
-    static constexpr int SC = ((L + L / 32 + 15) / 16) * 16 + 2;
+    // line stride in shared memory (complex elements): the swizzled length rounded
+    // to 16, plus an offset that puts the lines met by one half-warp on distinct
+    // banks: a column CTA has lanes c = 0..TX-1 on TX lines (offset 2 per line,
+    // the lane's p adds 0 or 1); a row CTA has P lanes per line (offset P).
+    static constexpr int SC = ((L + L / 32 + 15) / 16) * 16 + (ROWS ? (P % 16) : 2);
     __device__ static __forceinline__ int sw(int i) { return i + (i >> 5); }
 
     template <int Ns>
@@ -103,22 +108,81 @@ struct RegFFT {
 
 __device__ __forceinline__ int fold_idx(int i, int M) { return (M > 0 && 2 * i > M) ? M - i : i; }
 
+// asynchronous global -> shared copies of single elements (LDGSTS), so the
+// folded Green's values of a fused pass arrive while the forward DFT runs
+template <int B>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem_src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// folded Green's values staged per column: L/2 + 1 per column, row stride
+// = 4 (mod 32) elements so the multiply's reads hit distinct banks
+template <int L>
+struct GStage {
+    static constexpr int N = L / 2 + 1;
+    static constexpr int S = ((N + 31) / 32) * 32 + 4;
+};
+
 // ---------------------------------------------------------------- columns
 // MODE 0: forward DFT, 1: inverse DFT, 2: forward, Green multiply, inverse
+// Fused passes visit the outer index in mirror pairs (0, 1, M-1, 2, M-2, ...,
+// M/2) when the Green's function is folded along it, so the folded Green slab
+// read for o is read again for M-o while it is still in L2.
+__device__ __forceinline__ int mirror_order(int by, int nouter, int fold) {
+    if (fold != nouter || fold < 4) return by;
+    if (by == 0) return 0;
+    if (by == nouter - 1) return nouter / 2;
+    const int m = (by + 1) >> 1;
+    return (by & 1) ? m : nouter - m;
+}
+
+// resident threads per SM the register budget is sized for (2 CTAs of 256
+// threads for a fused or FP64 pass, 3 otherwise): the passes are bound by
+// memory, and more resident lines overlap one CTA's loads with another's
+// arithmetic
+#ifndef FLB_COL_THREADS_PER_SM
+#define FLB_COL_THREADS_PER_SM 768
+#endif
+#ifndef FLB_FUSED_THREADS_PER_SM
+#define FLB_FUSED_THREADS_PER_SM 512
+#endif
+template <typename T, int THREADS, int MODE>
+struct ColOcc {
+    static constexpr int per_sm = (MODE == 2 || sizeof(T) == 8) ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM;
+    static constexpr int want = per_sm / (THREADS < 64 ? 64 : THREADS);
+    static constexpr int blocks = want < 1 ? 1 : want;
+};
+
 template <typename T, int L, int R1, int TX, int MODE>
-__global__ void __launch_bounds__(TX * (L / R1)) col_dft_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), (ColOcc<T, TX * (L / R1), MODE>::blocks)) col_dft_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
     const int c = threadIdx.x % TX, p = threadIdx.x / TX;
     const int x = blockIdx.x * TX + c;
-    const int o = blockIdx.y;
+    const int o = (MODE == 2) ? mirror_order(blockIdx.y, a.nouter, a.f_outer) : (int)blockIdx.y;
     const int comp = blockIdx.z;
     const bool valid = x < a.nx;
     const C* in = reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x;
     C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x;
     const C* tw = reinterpret_cast<const C*>(a.tw);
+    T* gs = reinterpret_cast<T*>(sm + TX * F::SC);
+    if constexpr (MODE == 2) {
+        // the host guarantees fold length L along the line and L * g_line < 2^31
+        const T* g = reinterpret_cast<const T*>(a.green) + (int64_t)fold_idx(o, a.f_outer) * a.g_outer;
+        const int gl = (int)a.g_line;
+        for (int e = threadIdx.x; e < TX * GStage<L>::N; e += TX * F::P) {
+            const int cc = e % TX, j = e / TX, xx = blockIdx.x * TX + cc;
+            T* dst = gs + cc * GStage<L>::S + j;
+            if (xx < a.nx) cp_async<sizeof(T)>(dst, g + (int64_t)fold_idx(xx, a.f_x) * a.g_x + j * gl);
+            else *dst = (T)0;
+        }
+        cp_async_commit();
+    }
     C v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
@@ -128,16 +192,22 @@ __global__ void __launch_bounds__(TX * (L / R1)) col_dft_kernel(const ColArgs a)
     C* line = sm + c * F::SC;
     F::fft(v, line, p, tw, MODE == 1);
     if constexpr (MODE == 2) {
-        const T* g = reinterpret_cast<const T*>(a.green);
-        const int64_t gb = (int64_t)fold_idx(x < a.nx ? x : 0, a.f_x) * a.g_x + (int64_t)fold_idx(o, a.f_outer) * a.g_outer;
+        cp_async_wait_all();
+        __syncthreads();
+        const T* gc = gs + c * GStage<L>::S;
         const T nf = (T)a.normfact;
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
             const int k = p + F::P * r;
-            const T gv = g[gb + (int64_t)fold_idx(k, a.f_line) * a.g_line] * nf;
+            const T gv = gc[2 * k > L ? L - k : k] * nf;
             v[r] = mkc(v[r].x * gv, v[r].y * gv);
         }
-        F::fft(v, line, p, tw, true);
+        // a laundered copy of the table pointer: the compiler cannot merge the second
+        // DFT's twiddle loads with the first's, so those stay out of registers
+        // during the multiply
+        const C* tw2 = tw;
+        asm("" : "+l"(tw2));
+        F::fft(v, line, p, tw2, true);
     }
     if (valid) {
 #pragma unroll
@@ -151,7 +221,7 @@ __global__ void __launch_bounds__(TX * (L / R1)) col_dft_kernel(const ColArgs a)
 // ---------------------------------------------------------------- rows: r2c
 template <typename T, int LH, int R1, int TR>
 __global__ void __launch_bounds__(TR * (LH / R1)) row_r2c_kernel(const RowArgs a) {
-    using F = RegFFT<T, LH, R1>;
+    using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     constexpr int L = 2 * LH;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -221,7 +291,7 @@ __global__ void __launch_bounds__(TR * (LH / R1)) row_r2c_kernel(const RowArgs a
 // ---------------------------------------------------------------- rows: c2r
 template <typename T, int LH, int R1, int TR>
 __global__ void __launch_bounds__(TR * (LH / R1)) row_c2r_kernel(const RowArgs a) {
-    using F = RegFFT<T, LH, R1>;
+    using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -283,7 +353,7 @@ __global__ void __launch_bounds__(TR * (LH / R1)) row_c2r_kernel(const RowArgs a
 template <typename T, int L, int R1, int TX, int MODE>
 static cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, L, R1>;
-    const size_t smem = (size_t)TX * F::SC * sizeof(typename CT<T>::C);
+    const size_t smem = (size_t)TX * F::SC * sizeof(typename CT<T>::C) + (MODE == 2 ? (size_t)TX * GStage<L>::S * sizeof(T) : 0);
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(col_dft_kernel<T, L, R1, TX, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -327,7 +397,7 @@ cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncom
 
 template <typename T, int LH, int R1, bool C2R>
 static cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, LH, R1>;
+    using F = RegFFT<T, LH, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem = (size_t)TR * F::SC * sizeof(typename CT<T>::C);
     static bool attr = false;

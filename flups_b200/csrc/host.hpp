@@ -168,7 +168,9 @@ struct Solver {
     flb::LineStage stage_forward(const flb::DirPlan& p, int ip, bool f64);
     flb::LineStage stage_backward(const flb::DirPlan& p, const flb::DirPlan& pf, int ip, bool f64);
     flb::PassArgs base_pass(int axis, const ArrState& src, int ncomp, int lda_spec);
-    void set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s) const;
+    void set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s, bool pad = true) const;
+    int64_t row_pitch(const ArrState& s) const;             // x extent in memory (128-byte multiple)
+    size_t state_reals(int k, int nbatch) const;            // reals held by state k for nbatch right-hand sides
     void set_strides_user(int64_t str[3], int64_t& cstr) const;
     void fit_lines(flb::PassArgs& A, int elem_bytes) const;
     flb::MultSpec mult_spec(int type) const;

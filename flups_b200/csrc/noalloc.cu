@@ -99,10 +99,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
 
     // scratch layout: work arrays of the states the solve passes through, then twiddle tables
     size_t need[2] = {0, 0};
-    for (int k = 1; k < s->ndim; ++k) {
-        const size_t e = (size_t)s->st[k].n[0] * s->st[k].n[1] * s->st[k].n[2] * (s->st[k].cplx ? 2 : 1) * s->lda;
-        need[(k - 1) % 2] = std::max(need[(k - 1) % 2], e * es);
-    }
+    for (int k = 1; k < s->ndim; ++k) need[(k - 1) % 2] = std::max(need[(k - 1) % 2], s->state_reals(k, 1) * es);
     size_t off = 0;
     void* wb[2] = {nullptr, nullptr};
     for (int b = 0; b < 2; ++b) {

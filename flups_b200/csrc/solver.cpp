@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -287,11 +288,25 @@ LineStage Solver::stage_backward(const DirPlan& p, const DirPlan& pf, int ip, bo
     return S;
 }
 
-void Solver::set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s) const {
+// Work arrays keep every x row on a 128-byte boundary (the x extent, e.g. N+1
+// complex after an r2c, is padded in memory; the padding is never read or
+// written), so that the 32-byte sectors of a warp's row segment are whole.
+int64_t Solver::row_pitch(const ArrState& s) const {
+    const int64_t eb = (int64_t)(precision == 64 ? 8 : 4) * (s.cplx ? 2 : 1);
+    const int64_t q = std::max<int64_t>(1, 128 / eb);
+    return ((int64_t)s.n[0] + q - 1) / q * q;
+}
+
+size_t Solver::state_reals(int k, int nbatch) const {
+    return (size_t)row_pitch(st[k]) * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch;
+}
+
+void Solver::set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s, bool pad) const {
+    const int64_t px = pad ? row_pitch(s) : s.n[0];
     str[0] = 1;
-    str[1] = s.n[0];
-    str[2] = (int64_t)s.n[0] * s.n[1];
-    cstr = (int64_t)s.n[0] * s.n[1] * s.n[2];
+    str[1] = px;
+    str[2] = px * s.n[1];
+    cstr = px * s.n[1] * s.n[2];
 }
 
 void Solver::set_strides_user(int64_t str[3], int64_t& cstr) const {
@@ -389,6 +404,7 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
         // columns: complex DFT, working precision in and out, x contiguous
         if (k0 != LK_C2C || !S0.in_cplx || !S0.out_cplx || in_f64 != f64 || out_f64 != f64) return 0;
         if (A.fused && (A.st[1].spec[0].kind != LK_C2C || A.st[1].M != S0.M || A.mult.mode != 1)) return 0;
+        if (A.fused && (A.mult.gfold[A.axis] != S0.M || (int64_t)S0.M * A.mult.gstr[A.axis] >= (int64_t)INT32_MAX)) return 0;
         if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
         const int L = S0.M;
         if (!fast_col_supported(L) || A.n_src > L) return 0;
@@ -722,8 +738,8 @@ void Solver::compute_green() {
         S.n_store = S.n_o;
         S.tw = nullptr;
         A.st[0] = S;
-        set_strides_internal(A.in_str, A.in_cstr, cur);
-        set_strides_internal(A.out_str, A.out_cstr, nxt);
+        set_strides_internal(A.in_str, A.in_cstr, cur, false);
+        set_strides_internal(A.out_str, A.out_cstr, nxt, false);
         A.in = gb[cb];
         A.out = gb[1 - cb];
         fit_lines(A, sizeof(double));
@@ -746,11 +762,12 @@ void Solver::compute_green() {
     }
     for (int d = 0; d < 3; ++d)
         FLB_CHECK(spec_n[d] == st[ndim].n[d], "Topo of Green has to be the same as Topo of field");
-    gstr[0] = 1;
-    gstr[1] = gfold_n[0];
-    gstr[2] = (int64_t)gfold_n[0] * gfold_n[1];
     const bool f64 = (precision == 64);
-    const size_t gsz = (size_t)gfold_n[0] * gfold_n[1] * gfold_n[2];
+    const int64_t gq = f64 ? 16 : 32;  // rows of the folded spectrum on 128-byte boundaries
+    gstr[0] = 1;
+    gstr[1] = ((int64_t)gfold_n[0] + gq - 1) / gq * gq;
+    gstr[2] = gstr[1] * gfold_n[1];
+    const size_t gsz = (size_t)gstr[2] * gfold_n[2];
     if (dry) return;
     if (green) cudaFree(green);
     check_cuda(cudaMalloc(&green, gsz * (f64 ? 8 : 4)), "Green spectrum");
@@ -812,7 +829,7 @@ void Solver::ensure_buffers(int nbatch) {
         size_t need = 0;
         for (int k = 1; k < ndim; ++k) {
             if ((k - 1) % 2 != b) continue;
-            need = std::max(need, (size_t)st[k].n[0] * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch);
+            need = std::max(need, state_reals(k, nbatch));
         }
         if (need > buf_elems[b]) {
             if (buf[b]) cudaFree(buf[b]);
@@ -831,11 +848,11 @@ size_t Solver::device_bytes(int nbatch) const {
         size_t need = 0;
         for (int k = 1; k < ndim; ++k) {
             if ((k - 1) % 2 != b) continue;
-            need = std::max(need, (size_t)st[k].n[0] * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch);
+            need = std::max(need, state_reals(k, nbatch));
         }
         total += need * es;
     }
-    total += (size_t)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
+    total += (size_t)gstr[2] * gfold_n[2] * es;
     return total;
 }
 

@@ -74,7 +74,8 @@ def test_no_device_fails_loudly():
         "from flups_b200 import pyflups as pf\n"
         "t = pf.Topology(0, 1, [8, 8, 8])\n"
         "B = pf.BoundaryType\n"
-        "s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1/8]*3, [1.0]*3)\n" % str(ROOT)
+        "s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1/8]*3, [1.0]*3)\n"
+        "s.setup()\n" % str(ROOT)
     )
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True)
     assert r.returncode != 0
