@@ -171,6 +171,7 @@ static void timed_solve(Solver* s, double* field, double* rhs, int type, int nba
 }
 
 void flups_solve(Solver* s, double* field, double* rhs, const FLUPS_SolverType type) { timed_solve(s, field, rhs, type, 1); }
+void flups_synchronize(Solver* s) { s->check_cuda(cudaStreamSynchronize(s->stream), "synchronize"); }
 void flups_solve_rot(Solver* s, double* field, double* rhs) { timed_solve(s, field, rhs, ROT, 1); }
 void flups_solve_batch(Solver* s, double* field, double* rhs, int nbatch, int type) { timed_solve(s, field, rhs, type, nbatch); }
 

@@ -82,9 +82,13 @@ template <typename C> __device__ __forceinline__ void dft16(C* v) {
     for (int j2 = 1; j2 < 4; ++j2) {
 #pragma unroll
         for (int k1 = 1; k1 < 4; ++k1) {
-            S c, s;
-            w16<S>(j2 * k1, c, s);
-            v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, s));
+            if (j2 * k1 == 4) {
+                v[j2 + 4 * k1] = cmul_mi(v[j2 + 4 * k1]);
+            } else {
+                S c, s;
+                w16<S>(j2 * k1, c, s);
+                v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, s));
+            }
         }
     }
     C t[16];
@@ -137,9 +141,106 @@ template <typename C> __device__ __forceinline__ void dft32(C* v) {
     for (int n1 = 1; n1 < 4; ++n1) {
 #pragma unroll
         for (int k2 = 1; k2 < 8; ++k2) {
-            S c, s;
-            w32<S>(n1 * k2, c, s);
-            v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, s));
+            if (n1 * k2 == 8) {
+                v[n1 + 4 * k2] = cmul_mi(v[n1 + 4 * k2]);
+            } else {
+                S c, s;
+                w32<S>(n1 * k2, c, s);
+                v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, s));
+            }
+        }
+    }
+    C t[32];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        C a0 = v[0 + 4 * k2], a1 = v[1 + 4 * k2], a2 = v[2 + 4 * k2], a3 = v[3 + 4 * k2];
+        dft4(a0, a1, a2, a3);
+        t[k2 + 0] = a0; t[k2 + 8] = a1; t[k2 + 16] = a2; t[k2 + 24] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = t[i];
+}
+
+// Pruned butterflies for inputs whose upper half is zero (a zero-padded
+// line): the additions with the zero half are skipped.
+template <typename C> __device__ __forceinline__ void dft2z(C* v) { v[1] = v[0]; }
+
+// dft4 with a2 = a3 = 0
+template <typename C> __device__ __forceinline__ void dft4z(C& a0, C& a1, C& a2, C& a3) {
+    const C t = a0, u = a1, w = cmul_mi(a1);
+    a0 = cadd(t, u);
+    a2 = csub(t, u);
+    a1 = cadd(t, w);
+    a3 = csub(t, w);
+}
+template <typename C> __device__ __forceinline__ void dft4z(C* v) { dft4z(v[0], v[1], v[2], v[3]); }
+
+template <typename C> __device__ __forceinline__ void dft8z(C* v) {
+    using S = decltype(v[0].x);
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4z(e0, e1, e2, e3);
+    dft4z(o0, o1, o2, o3);
+    const S r2 = (S)FLB_R2;
+    o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);
+    o2 = cmul_mi(o2);
+    o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+template <typename C> __device__ __forceinline__ void dft16z(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int j2 = 0; j2 < 4; ++j2) dft4z(v[j2], v[j2 + 4], v[j2 + 8], v[j2 + 12]);
+#pragma unroll
+    for (int j2 = 1; j2 < 4; ++j2) {
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) {
+            if (j2 * k1 == 4) {
+                v[j2 + 4 * k1] = cmul_mi(v[j2 + 4 * k1]);
+            } else {
+                S c, s;
+                w16<S>(j2 * k1, c, s);
+                v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, s));
+            }
+        }
+    }
+    C t[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        C a0 = v[0 + 4 * k1], a1 = v[1 + 4 * k1], a2 = v[2 + 4 * k1], a3 = v[3 + 4 * k1];
+        dft4(a0, a1, a2, a3);
+        t[k1 + 0] = a0; t[k1 + 4] = a1; t[k1 + 8] = a2; t[k1 + 12] = a3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = t[i];
+}
+
+template <typename C> __device__ __forceinline__ void dft32z(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) {
+        C a[8];
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) a[n2] = v[n1 + 4 * n2];
+        dft8z(a);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) v[n1 + 4 * k2] = a[k2];
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < 4; ++n1) {
+#pragma unroll
+        for (int k2 = 1; k2 < 8; ++k2) {
+            if (n1 * k2 == 8) {
+                v[n1 + 4 * k2] = cmul_mi(v[n1 + 4 * k2]);
+            } else {
+                S c, s;
+                w32<S>(n1 * k2, c, s);
+                v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, s));
+            }
         }
     }
     C t[32];

@@ -14,7 +14,7 @@ struct ColArgs {
     int64_t in_lstr, in_ostr, in_cstr;     // element strides: along line, outer, component
     int64_t out_lstr, out_ostr, out_cstr;
     int nouter;
-    const void* tw;         // W_L^q, q < L (working precision)
+    const void* tws;        // later-stage twiddle table of the L-point DFT (fast_stage_table)
     // fused multiply
     const void* green;
     int64_t g_x, g_line, g_outer;          // folded Green strides
@@ -32,12 +32,36 @@ struct RowArgs {
     int64_t in_s1, in_s2, in_cstr;   // element strides of rows (i1, i2) and component
     int64_t out_s1, out_s2, out_cstr;
     int in_f64, out_f64;
-    const void* tw;         // W_L^q, q < L (L = 2 * Lh)
-    const void* twh;        // W_Lh^q, q < Lh
+    const void* tw;         // W_L^q, q < L (L = 2 * Lh): the real-to-half-length split
+    const void* tws;        // later-stage twiddle table of the Lh-point DFT (fast_stage_table)
 };
 
 bool fast_col_supported(int L);
 bool fast_row_supported(int L);
+
+// First radix of the register DFTs: 32 in FP32, 16 in FP64.
+int fast_radix1(int f64);
+// Complex entries of the later-stage twiddle table of an n-point register DFT.
+int fast_stage_table_len(int n, int f64);
+// Entry e of that table is W_M^q = exp(-2 pi i q / M); sets q and M.
+// Layout: one block of n entries per stage after the first (Ns = r1, r1*Rs, ...
+// with Rs = min(n/Ns, r1)); in a block, pair (b * Rs/2 + rp) * P + p (P = n/r1)
+// holds W_{Ns Rs}^{r k} for r = 2rp, 2rp+1 and k = (p + P b) mod Ns: the
+// twiddles of butterfly b of thread p, two per 16-byte (FP32) load.
+__host__ __device__ inline void fast_stage_exponent(int n, int r1, int e, int* q, int* M) {
+    const int P = n / r1;
+    const int s = e / n, w = e % n;
+    int Ns = r1;
+    for (int i = 0; i < s; ++i) Ns *= (n / Ns < r1) ? n / Ns : r1;
+    const int Rs = (n / Ns < r1) ? n / Ns : r1;
+    const int pair = w / 2, half = w % 2;
+    const int p = pair % P, t = pair / P;
+    const int rp = t % (Rs / 2), b = t / (Rs / 2);
+    const int r = 2 * rp + half, k = (p + P * b) % Ns;
+    *M = Ns * Rs;
+    *q = (int)(((long long)r * k) % (Ns * Rs));
+}
+
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 

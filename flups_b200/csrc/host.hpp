@@ -130,6 +130,15 @@ struct Solver {
     std::map<int64_t, void*> twiddles;    // key: M * 2 + (precision == 64)
     double* stage_in = nullptr;           // device staging for host rhs/field
     size_t stage_elems = 0;
+    // host-array solves: copies in slabs along the last forward direction,
+    // overlapped with the passes of the other slabs (and, with async, with the
+    // copies of the previous and next solve)
+    static constexpr int kSlabs = 8;
+    double* stage_out = nullptr;          // device staging for a host field (separate from stage_in)
+    size_t stage_out_elems = 0;
+    cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
+    cudaEvent_t ev_in[kSlabs] = {}, ev_fwd[kSlabs] = {}, ev_bwd[kSlabs] = {}, ev_out[kSlabs] = {};
+    int slab_dim = -1, slab_lo = 0, slab_hi = 0;   // restriction run_pass applies to non-fused passes
     double* inner = nullptr;              // spectral buffer of the advanced API (doubles)
     Topology* topo_spec = nullptr;
     Topology* topo_inner_phys = nullptr;
@@ -162,7 +171,10 @@ struct Solver {
     void compute_green();
     const void* twiddle(int M, bool f64);
     const void* twiddle_plain(int L, bool f64);   // W_L^q, q < L
+    const void* stage_table(int n, bool f64);     // later-stage twiddles of an n-point register DFT
     int fast_kind(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64) const;  // 0 none, 1 column, 2 row
+    // arguments of a fast launch, all but the twiddle tables; mode of a column pass
+    void fast_args(const flb::PassArgs& A, int kind, bool in_f64, bool out_f64, flb::ColArgs& c, flb::RowArgs& r, int& mode) const;
     void launch_fast(const flb::PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64);
     void ensure_buffers(int nbatch);
     flb::LineStage stage_forward(const flb::DirPlan& p, int ip, bool f64);
@@ -178,6 +190,11 @@ struct Solver {
     void collect_timing();
     void check_cuda(cudaError_t e, const char* what);
     void do_fft_forward(const double* user_in, int nbatch);
+    void do_fused(int type, int nbatch);
+    void do_backward(double* user_out, int type, int nbatch);
     void do_fft_backward_fused(double* user_out, int type, int nbatch);
+    bool streamed_ok() const;
+    void solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch);
+    void restrict_slab(flb::PassArgs& A, bool in_f64, bool out_f64) const;
     std::string plan_json(int type, int nbatch);
 };

@@ -42,20 +42,25 @@ static void* g_noalloc_ptr[FLUPS_NOALLOC_MAX_DEVICES] = {nullptr};
 
 using namespace flb;
 
-// exp(-2 pi i q / n) for q < n, FP64 sincospi, stored in the working precision
-__global__ void noalloc_twiddle_kernel(void* out, int n, int f64) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+// exp(-2 pi i q / n) for q < n (stage == 0), or the later-stage table of an
+// n-point register DFT (stage == 1); FP64 sincospi, stored in the working precision
+__global__ void noalloc_twiddle_kernel(void* out, int n, int stage, int len, int r1, int f64) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < len; e += gridDim.x * blockDim.x) {
+        int q = e, M = n;
+        if (stage) fast_stage_exponent(n, r1, e, &q, &M);
         double s, c;
-        sincospi(-2.0 * (double)q / (double)n, &s, &c);
-        if (f64) reinterpret_cast<double2*>(out)[q] = make_double2(c, s);
-        else reinterpret_cast<float2*>(out)[q] = make_float2((float)c, (float)s);
+        sincospi(-2.0 * (double)q / (double)M, &s, &c);
+        if (f64) reinterpret_cast<double2*>(out)[e] = make_double2(c, s);
+        else reinterpret_cast<float2*>(out)[e] = make_float2((float)c, (float)s);
     }
 }
 
 namespace {
 
 struct TwSlot {
-    int n;        // table length (complex entries)
+    int n;        // transform length
+    int stage;    // 0: W_n^q table, 1: later-stage table of an n-point register DFT
+    int len;      // complex entries
     size_t off;   // byte offset in the scratch array
 };
 
@@ -130,13 +135,14 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     s->buf[0] = keep[0];
     s->buf[1] = keep[1];
 
-    // twiddle tables: one per distinct length
+    // twiddle tables: one per distinct (length, layout)
     std::vector<TwSlot> slots;
-    auto slot_for = [&](int n) -> size_t {
+    auto slot_for = [&](int n, int stage) -> size_t {
         for (const TwSlot& t : slots)
-            if (t.n == n) return t.off;
-        TwSlot t{n, off};
-        off = align256(off + (size_t)n * 2 * es);
+            if (t.n == n && t.stage == stage) return t.off;
+        const int len = stage ? std::max(1, fast_stage_table_len(n, f64 ? 1 : 0)) : n;
+        TwSlot t{n, stage, len, off};
+        off = align256(off + (size_t)len * 2 * es);
         slots.push_back(t);
         return t.off;
     };
@@ -146,10 +152,12 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
         const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
         kinds[i] = s->fast_kind(A, f64, in64, out64);
         if (kinds[i] == 0) {
-            for (int sg = 0; sg <= A.fused; ++sg) slot_for(2 * A.st[sg].M);
+            for (int sg = 0; sg <= A.fused; ++sg) slot_for(2 * A.st[sg].M, 0);
+        } else if (kinds[i] == 1) {
+            slot_for(A.st[0].M, 1);
         } else {
-            slot_for(A.st[0].M);
-            if (kinds[i] == 2) slot_for(A.st[0].M / 2);
+            slot_for(A.st[0].M, 0);
+            slot_for(A.st[0].M / 2, 1);
         }
     }
     if (off > FLUPS_NOALLOC_SCRATCH_BYTES) {
@@ -161,71 +169,31 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
 
     cudaStream_t st = s->stream;
     for (const TwSlot& t : slots) {
-        const int nb = std::min(1184, (t.n + 255) / 256);
-        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, f64 ? 1 : 0);
+        const int nb = std::min(1184, (t.len + 255) / 256);
+        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, fast_radix1(f64 ? 1 : 0), f64 ? 1 : 0);
     }
-    auto tw_of = [&](int n) { return (const void*)(base + slot_for(n)); };
+    auto tw_of = [&](int n, int stage) { return (const void*)(base + slot_for(n, stage)); };
     for (size_t i = 0; i < passes.size(); ++i) {
         PassArgs& A = passes[i];
         const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
         cudaError_t e = cudaSuccess;
         if (kinds[i] == 0) {
-            for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M);
+            for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M, 0);
             e = launch_line_pass(A, f64 ? 1 : 0, in64 ? 1 : 0, out64 ? 1 : 0, st);
-        } else if (kinds[i] == 1) {
-            const LineStage& S0 = A.st[0];
-            const int L = S0.M;
-            const int b = (A.axis == 2) ? 1 : 2;
-            ColArgs c;
-            memset(&c, 0, sizeof(c));
-            c.in = A.in;
-            c.out = A.out;
-            c.nx = A.n_a;
-            c.nouter = A.n_b;
-            c.nin = A.n_src;
-            c.nout = A.st[A.fused ? 1 : 0].n_store;
-            c.in_lstr = A.in_str[A.axis];
-            c.in_ostr = A.in_str[b];
-            c.in_cstr = A.in_cstr;
-            c.out_lstr = A.out_str[A.axis];
-            c.out_ostr = A.out_str[b];
-            c.out_cstr = A.out_cstr;
-            c.tw = tw_of(L);
-            int mode = (S0.spec[0].sign > 0) ? 1 : 0;
-            if (A.fused) {
-                mode = 2;
-                c.green = A.mult.green;
-                c.g_x = A.mult.gstr[0];
-                c.g_line = A.mult.gstr[A.axis];
-                c.g_outer = A.mult.gstr[b];
-                c.f_x = A.mult.gfold[0];
-                c.f_line = A.mult.gfold[A.axis];
-                c.f_outer = A.mult.gfold[b];
-                c.normfact = A.mult.normfact;
-            }
-            e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
         } else {
-            const LineStage& S0 = A.st[0];
-            const int L = S0.M;
+            const int L = A.st[0].M;
+            ColArgs c;
             RowArgs r;
-            memset(&r, 0, sizeof(r));
-            r.in = A.in;
-            r.out = A.out;
-            r.n1 = A.n_a;
-            r.nrows = A.n_a * A.n_b;
-            r.nin = A.n_src;
-            r.nout = S0.n_store;
-            r.in_s1 = A.in_str[1];
-            r.in_s2 = A.in_str[2];
-            r.in_cstr = A.in_cstr;
-            r.out_s1 = A.out_str[1];
-            r.out_s2 = A.out_str[2];
-            r.out_cstr = A.out_cstr;
-            r.in_f64 = in64;
-            r.out_f64 = out64;
-            r.tw = tw_of(L);
-            r.twh = tw_of(L / 2);
-            e = launch_fast_row(f64 ? 1 : 0, S0.spec[0].kind == LK_C2R, L, r, A.ncomp, st);
+            int mode = 0;
+            s->fast_args(A, kinds[i], in64, out64, c, r, mode);
+            if (kinds[i] == 1) {
+                c.tws = tw_of(L, 1);
+                e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
+            } else {
+                r.tw = tw_of(L, 0);
+                r.tws = tw_of(L / 2, 1);
+                e = launch_fast_row(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, st);
+            }
         }
         if (e != cudaSuccess) {
             s->last_error = (int)e;

@@ -152,11 +152,27 @@ void Solver::dry_run(DirPlan p[3]) {
 }
 
 Solver::~Solver() {
+    if (h2d_stream) {
+        // copies of an async solve may still be in flight
+        cudaStreamSynchronize(h2d_stream);
+        cudaStreamSynchronize(d2h_stream);
+    }
     for (auto& b : buf)
         if (b) cudaFree(b);
     if (green) cudaFree(green);
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
+    if (stage_out) cudaFree(stage_out);
+    if (h2d_stream) {
+        for (int k = 0; k < kSlabs; ++k) {
+            cudaEventDestroy(ev_in[k]);
+            cudaEventDestroy(ev_fwd[k]);
+            cudaEventDestroy(ev_bwd[k]);
+            cudaEventDestroy(ev_out[k]);
+        }
+        cudaStreamDestroy(h2d_stream);
+        cudaStreamDestroy(d2h_stream);
+    }
     if (inner) cudaFree(inner);
     for (auto e : ev) cudaEventDestroy(e);
     delete topo_spec;
@@ -408,6 +424,8 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
         if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
         const int L = S0.M;
         if (!fast_col_supported(L) || A.n_src > L) return 0;
+        // 32-bit element offsets along a line
+        if ((int64_t)L * A.in_str[A.axis] >= (int64_t)INT32_MAX || (int64_t)L * A.out_str[A.axis] >= (int64_t)INT32_MAX) return 0;
         const LineStage& SL = A.st[A.fused ? 1 : 0];
         if (SL.n_store > L) return 0;
         if (!A.fused && S0.n_o != L) return 0;
@@ -432,13 +450,13 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
     return 0;
 }
 
-void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64) {
+void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, ColArgs& c, RowArgs& r, int& mode) const {
     const LineStage& S0 = A.st[0];
-    const int L = S0.M;
     const int b = (A.axis == 2) ? 1 : 2;
+    memset(&c, 0, sizeof(c));
+    memset(&r, 0, sizeof(r));
+    mode = 0;
     if (kind == 1) {
-        ColArgs c;
-        memset(&c, 0, sizeof(c));
         c.in = A.in;
         c.out = A.out;
         c.nx = A.n_a;
@@ -451,8 +469,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         c.out_lstr = A.out_str[A.axis];
         c.out_ostr = A.out_str[b];
         c.out_cstr = A.out_cstr;
-        c.tw = twiddle_plain(L, f64);
-        int mode = (S0.spec[0].sign > 0) ? 1 : 0;
+        mode = (S0.spec[0].sign > 0) ? 1 : 0;
         if (A.fused) {
             mode = 2;
             c.green = A.mult.green;
@@ -464,11 +481,8 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
             c.f_outer = A.mult.gfold[b];
             c.normfact = A.mult.normfact;
         }
-        check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
         return;
     }
-    RowArgs r;
-    memset(&r, 0, sizeof(r));
     r.in = A.in;
     r.out = A.out;
     r.n1 = A.n_a;
@@ -483,9 +497,49 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     r.out_cstr = A.out_cstr;
     r.in_f64 = in_f64;
     r.out_f64 = out_f64;
+}
+
+void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64) {
+    const int L = A.st[0].M;
+    ColArgs c;
+    RowArgs r;
+    int mode = 0;
+    fast_args(A, kind, in_f64, out_f64, c, r, mode);
+    if (kind == 1) {
+        c.tws = stage_table(L, f64);
+        check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
+        return;
+    }
     r.tw = twiddle_plain(L, f64);
-    r.twh = twiddle_plain(L / 2, f64);
-    check_cuda(launch_fast_row(f64, S0.spec[0].kind == LK_C2R, L, r, A.ncomp, stream), "row DFT launch");
+    r.tws = stage_table(L / 2, f64);
+    check_cuda(launch_fast_row(f64, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, stream), "row DFT launch");
+}
+
+const void* Solver::stage_table(int n, bool f64) {
+    const int64_t key = ((int64_t)1 << 40) + (int64_t)n * 2 + (f64 ? 1 : 0);
+    auto it = twiddles.find(key);
+    if (it != twiddles.end()) return it->second;
+    const int len = fast_stage_table_len(n, f64 ? 1 : 0), r1 = fast_radix1(f64 ? 1 : 0);
+    std::vector<double> w(2 * (size_t)std::max(len, 1), 0.0);
+    for (int e = 0; e < len; ++e) {
+        int q = 0, M = 1;
+        fast_stage_exponent(n, r1, e, &q, &M);
+        const long double a = -2.0L * (long double)M_PI * (long double)q / (long double)M;
+        w[2 * e] = (double)cosl(a);
+        w[2 * e + 1] = (double)sinl(a);
+    }
+    void* d = nullptr;
+    if (f64) {
+        check_cuda(cudaMalloc(&d, w.size() * sizeof(double)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice), "twiddle upload");
+    } else {
+        std::vector<float> wf(w.size());
+        for (size_t i = 0; i < w.size(); ++i) wf[i] = (float)w[i];
+        check_cuda(cudaMalloc(&d, wf.size() * sizeof(float)), "twiddle allocation");
+        check_cuda(cudaMemcpy(d, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice), "twiddle upload");
+    }
+    twiddles[key] = d;
+    return d;
 }
 
 const void* Solver::twiddle_plain(int L, bool f64) {
@@ -512,8 +566,24 @@ const void* Solver::twiddle_plain(int L, bool f64) {
     return d;
 }
 
+// Restrict a pass to the slab [slab_lo, slab_hi) of dimension slab_dim (not
+// its line axis): both arrays start at the slab, the lines outside it are skipped.
+void Solver::restrict_slab(PassArgs& A, bool in_f64, bool out_f64) const {
+    const int a = (A.axis == 0) ? 1 : 0;
+    const int d = slab_dim;
+    const int64_t lo = slab_lo;
+    const int64_t ein = (in_f64 ? 8 : 4) * (A.st[0].in_cplx ? 2 : 1);
+    const int64_t eout = (out_f64 ? 8 : 4) * (A.st[A.fused ? 1 : 0].out_cplx ? 2 : 1);
+    A.in = (const char*)A.in + lo * A.in_str[d] * ein;
+    A.out = (char*)A.out + lo * A.out_str[d] * eout;
+    if (d == a) A.n_a = slab_hi - slab_lo;
+    else A.n_b = slab_hi - slab_lo;
+    A.nlines = (int64_t)A.n_a * A.n_b;
+}
+
 void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, const char* name) {
     PassArgs A = Ain;
+    if (slab_dim >= 0 && !A.fused && A.axis != slab_dim) restrict_slab(A, in_f64, out_f64);
     const int fk = fast_kind(A, f64, in_f64, out_f64);
     if (dry) {
         dry_passes.push_back(A);
@@ -888,6 +958,11 @@ void Solver::do_fft_forward(const double* user_in, int nbatch) {
 }
 
 void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
+    do_fused(type, nbatch);
+    do_backward(user_out, type, nbatch);
+}
+
+void Solver::do_fused(int type, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const int ipl = ndim - 1;
@@ -920,6 +995,11 @@ void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
             run_pass(A, f64, f64, f64, "fused");
         }
     }
+}
+
+void Solver::do_backward(double* user_out, int type, int nbatch) {
+    const bool f64 = (precision == 64);
+    const int es = f64 ? 8 : 4;
     for (int ip = ndim - 2; ip >= 0; --ip) {
         const DirPlan& p = (type == ROT) ? dif[ip] : bwd[ip];
         PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda * nbatch, lda);
@@ -951,6 +1031,10 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     ensure_buffers(nbatch);
     const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
     const bool dev_in = is_device_ptr(rhs), dev_out = is_device_ptr(field);
+    if ((!dev_in || !dev_out) && streamed_ok()) {
+        solve_streamed(field, rhs, !dev_in, !dev_out, type, nbatch);
+        return;
+    }
     double* din = rhs;
     double* dout = field;
     if (!dev_in || !dev_out) {
@@ -973,6 +1057,100 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
         check_cuda(cudaMemcpyAsync(field, dout, user_elems * sizeof(double), cudaMemcpyDeviceToHost, stream), "field download");
     }
     if (!async || !dev_out || !dev_in) check_cuda(cudaStreamSynchronize(stream), "solve");
+    else check_cuda(cudaGetLastError(), "solve");
+}
+
+// ---------------------------------------------------------------- host arrays, streamed
+// The passes before and after the fused one work on lines of the other two
+// directions, so slabs of the last forward direction are independent there:
+// slab k of rhs is uploaded while slab k-1 is transformed, and slab k of the
+// result is downloaded while slab k+1 is transformed back.  Uploads and
+// downloads use their own streams and staging arrays, so with async the
+// upload of the next solve overlaps the download of this one.
+bool Solver::streamed_ok() const {
+    // slabs along z are contiguous in the user layout (x fastest)
+    return !timing && ndim == 3 && fwd[ndim - 1].dim == 2 && st[0].n[2] >= 2;
+}
+
+void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch) {
+    const int d = 2;
+    const int nd = st[0].n[d];
+    const int ns = std::min(kSlabs, nd);
+    const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
+    if (in_host && stage_elems < user_elems) {
+        if (stage_in) cudaFree(stage_in);
+        stage_in = nullptr;
+        check_cuda(cudaMalloc(&stage_in, user_elems * sizeof(double)), "staging buffer");
+        stage_elems = user_elems;
+    }
+    if (out_host && stage_out_elems < user_elems) {
+        if (stage_out) cudaFree(stage_out);
+        stage_out = nullptr;
+        check_cuda(cudaMalloc(&stage_out, user_elems * sizeof(double)), "staging buffer");
+        stage_out_elems = user_elems;
+    }
+    if (!h2d_stream) {
+        check_cuda(cudaStreamCreateWithFlags(&h2d_stream, cudaStreamNonBlocking), "copy stream");
+        check_cuda(cudaStreamCreateWithFlags(&d2h_stream, cudaStreamNonBlocking), "copy stream");
+        for (int k = 0; k < kSlabs; ++k) {
+            check_cuda(cudaEventCreateWithFlags(&ev_in[k], cudaEventDisableTiming), "event");
+            check_cuda(cudaEventCreateWithFlags(&ev_fwd[k], cudaEventDisableTiming), "event");
+            check_cuda(cudaEventCreateWithFlags(&ev_bwd[k], cudaEventDisableTiming), "event");
+            check_cuda(cudaEventCreateWithFlags(&ev_out[k], cudaEventDisableTiming), "event");
+        }
+    }
+    int64_t ustr[3], ucstr;
+    set_strides_user(ustr, ucstr);
+    const int ncomp = lda * nbatch;
+    double* din = in_host ? stage_in : rhs;
+    double* dout = out_host ? stage_out : field;
+    pass_idx = 0;
+    for (int k = 0; k < ns; ++k) {
+        const int lo = (int)((int64_t)k * nd / ns), hi = (int)((int64_t)(k + 1) * nd / ns);
+        if (in_host) {
+            // the previous solve's passes have read this slab of the staging array
+            check_cuda(cudaStreamWaitEvent(h2d_stream, ev_fwd[k], 0), "stream wait");
+            for (int c = 0; c < ncomp; ++c) {
+                const size_t off = (size_t)c * ucstr + (size_t)lo * ustr[d];
+                check_cuda(cudaMemcpyAsync(stage_in + off, rhs + off, (size_t)(hi - lo) * ustr[d] * sizeof(double),
+                                           cudaMemcpyHostToDevice, h2d_stream),
+                           "rhs upload");
+            }
+            check_cuda(cudaEventRecord(ev_in[k], h2d_stream), "event record");
+            check_cuda(cudaStreamWaitEvent(stream, ev_in[k], 0), "stream wait");
+        }
+        slab_dim = d;
+        slab_lo = lo;
+        slab_hi = hi;
+        do_fft_forward(din, nbatch);
+        slab_dim = -1;
+        check_cuda(cudaEventRecord(ev_fwd[k], stream), "event record");
+    }
+    do_fused(type, nbatch);
+    for (int k = 0; k < ns; ++k) {
+        const int lo = (int)((int64_t)k * nd / ns), hi = (int)((int64_t)(k + 1) * nd / ns);
+        // the previous solve's download of this slab of the staging array is done
+        if (out_host) check_cuda(cudaStreamWaitEvent(stream, ev_out[k], 0), "stream wait");
+        slab_dim = d;
+        slab_lo = lo;
+        slab_hi = hi;
+        do_backward(dout, type, nbatch);
+        slab_dim = -1;
+        if (out_host) {
+            check_cuda(cudaEventRecord(ev_bwd[k], stream), "event record");
+            check_cuda(cudaStreamWaitEvent(d2h_stream, ev_bwd[k], 0), "stream wait");
+            for (int c = 0; c < ncomp; ++c) {
+                const size_t off = (size_t)c * ucstr + (size_t)lo * ustr[d];
+                check_cuda(cudaMemcpyAsync(field + off, stage_out + off, (size_t)(hi - lo) * ustr[d] * sizeof(double),
+                                           cudaMemcpyDeviceToHost, d2h_stream),
+                           "field download");
+            }
+            check_cuda(cudaEventRecord(ev_out[k], d2h_stream), "event record");
+        }
+    }
+    // work queued later on the caller's stream sees the downloaded result
+    if (out_host) check_cuda(cudaStreamWaitEvent(stream, ev_out[ns - 1], 0), "stream wait");
+    if (!async) check_cuda(cudaStreamSynchronize(stream), "solve");
     else check_cuda(cudaGetLastError(), "solve");
 }
 

@@ -111,6 +111,7 @@ def load_library(path=None):
         "flups_set_precision": (None, [vp, c_int]),
         "flups_get_precision": (c_int, [vp]),
         "flups_set_async": (None, [vp, c_int]),
+        "flups_synchronize": (None, [vp]),
         "flups_get_last_error": (c_int, [vp]),
         "flups_get_device_bytes": (c_size_t, [vp, c_int]),
         "flups_b200_plan_json": (c_int, [vp, c_int, c_int, ctypes.c_char_p, c_int]),
@@ -254,6 +255,9 @@ class Solver:
 
     def set_async(self, flag):
         _lib.flups_set_async(self._solver, int(bool(flag)))
+
+    def synchronize(self):
+        _lib.flups_synchronize(self._solver)
 
     def setup(self, change_comm=False):
         _lib.flups_setup(self._solver, bool(change_comm))

@@ -32,9 +32,18 @@ int flups_get_precision(struct Solver* s);
  * reference counterpart; equivalent to nbatch calls of flups_solve. */
 void flups_solve_batch(struct Solver* s, double* field, double* rhs, int nbatch, int type);
 
-/* When set, flups_solve with device pointers returns without synchronising
- * the solver's stream (host pointers always synchronise).  Default 0. */
+/* When set, flups_solve returns once its work is queued on the solver's
+ * stream, without synchronising.  With host arrays the upload of rhs and the
+ * download of field run on the library's copy streams in slabs, overlapped
+ * with the transforms and with the copies of the previous and next solve;
+ * rhs and field must stay untouched until the solve is complete (for host
+ * arrays page-locked memory lets the copies run asynchronously).  Completion
+ * is ordered before later work on the solver's stream; flups_synchronize
+ * waits for it.  Default 0 (every call returns with its result in place). */
 void flups_set_async(struct Solver* s, int async);
+
+/* Wait for every solve queued on the solver's stream (async mode). */
+void flups_synchronize(struct Solver* s);
 
 /* Last CUDA error seen by the solver (0 = none).  No reference counterpart:
  * the reference aborts on every error (src/defines.hpp:301-304). */
