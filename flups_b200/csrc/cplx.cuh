@@ -14,6 +14,15 @@ __device__ __forceinline__ double2 mkc(double x, double y) { return make_double2
 
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc(a.x + b.x, a.y + b.y); }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc(a.x - b.x, a.y - b.y); }
+#ifndef FLB_PAIRED_FP32
+#define FLB_PAIRED_FP32 1
+#endif
+#if FLB_PAIRED_FP32 && defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+// FP32 complex additions as one paired instruction (per component the same
+// rounding as the scalar operation); a - b as b * (-1) + a, exact in the product
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+#endif
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -28,13 +37,17 @@ template <typename C> __device__ __forceinline__ void dft2(C* v) {
     v[1] = csub(t, v[1]);
 }
 
+// t -/+ i d, component by component (no swapped pair is formed)
+template <typename C> __device__ __forceinline__ C csub_i(C t, C d) { return mkc(t.x + d.y, t.y - d.x); }
+template <typename C> __device__ __forceinline__ C cadd_i(C t, C d) { return mkc(t.x - d.y, t.y + d.x); }
+
 template <typename C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
-    C t0 = cadd(a0, a2), t1 = csub(a0, a2);
-    C t2 = cadd(a1, a3), t3 = cmul_mi(csub(a1, a3));
+    const C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    const C t2 = cadd(a1, a3), d = csub(a1, a3);
     a0 = cadd(t0, t2);
     a2 = csub(t0, t2);
-    a1 = cadd(t1, t3);
-    a3 = csub(t1, t3);
+    a1 = csub_i(t1, d);  // t1 + (-i) d
+    a3 = cadd_i(t1, d);  // t1 - (-i) d
 }
 template <typename C> __device__ __forceinline__ void dft4(C* v) { dft4(v[0], v[1], v[2], v[3]); }
 
@@ -51,11 +64,10 @@ template <typename C> __device__ __forceinline__ void dft8(C* v) {
     dft4(o0, o1, o2, o3);
     const S r2 = (S)FLB_R2;
     o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);  // * W8^1
-    o2 = cmul_mi(o2);                                   // * W8^2
     o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // * W8^3
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
     v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[2] = csub_i(e2, o2); v[6] = cadd_i(e2, o2);       // o2 * W8^2 = -i o2
     v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
@@ -167,11 +179,11 @@ template <typename C> __device__ __forceinline__ void dft2z(C* v) { v[1] = v[0];
 
 // dft4 with a2 = a3 = 0
 template <typename C> __device__ __forceinline__ void dft4z(C& a0, C& a1, C& a2, C& a3) {
-    const C t = a0, u = a1, w = cmul_mi(a1);
+    const C t = a0, u = a1;
     a0 = cadd(t, u);
     a2 = csub(t, u);
-    a1 = cadd(t, w);
-    a3 = csub(t, w);
+    a1 = csub_i(t, u);
+    a3 = cadd_i(t, u);
 }
 template <typename C> __device__ __forceinline__ void dft4z(C* v) { dft4z(v[0], v[1], v[2], v[3]); }
 
@@ -183,11 +195,10 @@ template <typename C> __device__ __forceinline__ void dft8z(C* v) {
     dft4z(o0, o1, o2, o3);
     const S r2 = (S)FLB_R2;
     o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);
-    o2 = cmul_mi(o2);
     o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
     v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[2] = csub_i(e2, o2); v[6] = cadd_i(e2, o2);
     v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 

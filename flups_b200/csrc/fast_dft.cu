@@ -26,7 +26,6 @@
 #include "cplx.cuh"
 #include "fast_dft.h"
 #include "pass_desc.h"
-#include "vmem.cuh"
 
 namespace flb {
 
@@ -54,23 +53,15 @@ __device__ __forceinline__ void dftz(C* v) {
 template <typename T, bool SM> struct TwPair;
 template <bool SM> struct TwPair<float, SM> {
     __device__ static __forceinline__ void ld(const float2* p, float2& a, float2& b) {
-        float4 q;
-        if constexpr (SM) lds(smem_u32(p), q);
-        else q = __ldg(reinterpret_cast<const float4*>(p));
+        const float4 q = SM ? *reinterpret_cast<const float4*>(p) : __ldg(reinterpret_cast<const float4*>(p));
         a = make_float2(q.x, q.y);
         b = make_float2(q.z, q.w);
     }
 };
 template <bool SM> struct TwPair<double, SM> {
     __device__ static __forceinline__ void ld(const double2* p, double2& a, double2& b) {
-        if constexpr (SM) {
-            const unsigned u = smem_u32(p);
-            lds(u, a);
-            lds(u + 16, b);
-        } else {
-            a = __ldg(p);
-            b = __ldg(p + 1);
-        }
+        a = SM ? p[0] : __ldg(p);
+        b = SM ? p[1] : __ldg(p + 1);
     }
 };
 
@@ -111,13 +102,12 @@ struct RegFFT {
             const int j = p + P * b;
             if constexpr (MR % 32 == 0) {
                 // sw(j + r MR) = sw(j) + r (MR + MR/32) when MR is a multiple of 32
-                const unsigned s0 = smem_u32(sm + sw(j));
+                const C* s0 = sm + sw(j);
 #pragma unroll
-                for (int r = 0; r < Rs; ++r) lds(s0 + r * (MR + MR / 32) * (int)sizeof(C), t[b * Rs + r]);
+                for (int r = 0; r < Rs; ++r) t[b * Rs + r] = s0[r * (MR + MR / 32)];
             } else {
-                const unsigned s0 = smem_u32(sm);
 #pragma unroll
-                for (int r = 0; r < Rs; ++r) lds(s0 + sw(j + r * MR) * (int)sizeof(C), t[b * Rs + r]);
+                for (int r = 0; r < Rs; ++r) t[b * Rs + r] = sm[sw(j + r * MR)];
             }
             const C* tb = tws + 2 * (b * (Rs / 2) * P + p);
 #pragma unroll
@@ -141,13 +131,12 @@ struct RegFFT {
                 const int j = p + P * b;
                 const int base = (j / Ns) * Ns * Rs + (j % Ns);
                 if constexpr (Ns % 32 == 0) {
-                    const unsigned d0 = smem_u32(sm + sw(base));
+                    C* d0 = sm + sw(base);
 #pragma unroll
-                    for (int r = 0; r < Rs; ++r) sts(d0 + r * (Ns + Ns / 32) * (int)sizeof(C), t[b * Rs + r]);
+                    for (int r = 0; r < Rs; ++r) d0[r * (Ns + Ns / 32)] = t[b * Rs + r];
                 } else {
-                    const unsigned d0 = smem_u32(sm);
 #pragma unroll
-                    for (int r = 0; r < Rs; ++r) sts(d0 + sw(base + r * Ns) * (int)sizeof(C), t[b * Rs + r]);
+                    for (int r = 0; r < Rs; ++r) sm[sw(base + r * Ns)] = t[b * Rs + r];
                 }
             }
             __syncthreads();
@@ -168,9 +157,9 @@ struct RegFFT {
         if constexpr (P > 1) {
             __syncthreads();
             // sw(p R1 + k) = sw(p R1) + k for k < R1 <= 32
-            const unsigned d0 = smem_u32(sm + sw(p * R1));
+            C* d0 = sm + sw(p * R1);
 #pragma unroll
-            for (int k = 0; k < R1; ++k) sts(d0 + k * (int)sizeof(C), v[k]);
+            for (int k = 0; k < R1; ++k) d0[k] = v[k];
             __syncthreads();
             stages<R1>(v, sm, p, tws);
         }
@@ -293,15 +282,20 @@ struct Occ {
 };
 
 // ---------------------------------------------------------------- columns
-// MODE 0: forward DFT, 1: inverse DFT, 2: forward, Green multiply, inverse.
-// HALF: the line is zero-padded to L (nin = L/2, modes 0 and 2) and/or
-// truncated (nout = L/2, modes 1 and 2); otherwise nin/nout are tested.
+// Extent of the loaded / stored part of a line, known at compile time:
+enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
+// MODE 0: forward DFT (SH: loaded part; SH != ANY also means all L stored),
+//      1: inverse DFT (SH: stored part; SH != ANY also means all L loaded),
+//      2: forward, Green multiply, inverse (SH: loaded and stored part).
 // The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
-template <typename T, int L, int R1, int TX, int MODE, bool HALF>
+template <typename T, int L, int R1, int TX, int MODE, int SH>
 __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col_dft_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
-    constexpr bool HIN = HALF && MODE != 1, HOUT = HALF && MODE != 0;
+    constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
+    constexpr int OUTS = (MODE == 0) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
+    constexpr int NLD = (INS == SH_HALF) ? R1 / 2 : R1;  // registers loaded
+    constexpr int NST = (OUTS == SH_HALF) ? R1 / 2 : R1;  // registers stored
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
     const int c = threadIdx.x % TX, p = threadIdx.x / TX;
@@ -313,18 +307,21 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
     const C* tws = stage_twiddles<F>(a.tws, sm + TX * F::SC);
     T* gs = reinterpret_cast<T*>(sm + TX * F::SC + F::TW_SMEM);
     if constexpr (MODE == 2) stage_green<T, L, TX>(a, gs, o);
-    const C* in = reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr;
-    const int ls = F::P * (int)a.in_lstr;
+    // lanes outside the array read its first element and drop it (no branch)
+    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+                        : reinterpret_cast<const C*>(a.in);
+    const int ls = valid ? F::P * (int)a.in_lstr : 0;
     C v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
-        if (HIN && r >= R1 / 2) {
+        if (r >= NLD) {
             v[r] = mkc((T)0, (T)0);
+        } else if constexpr (INS != SH_ANY) {
+            const C t = in[r * ls];
+            v[r] = valid ? t : mkc((T)0, (T)0);
         } else {
-            // lanes outside the array load the array's first element and drop it (no branch)
-            const bool ok = valid && (HIN || p + F::P * r < a.nin);
-            C t;
-            ldg(ok ? in + r * ls : reinterpret_cast<const C*>(a.in), t);
+            const bool ok = valid && p + F::P * r < a.nin;
+            const C t = in[ok ? r * ls : 0];
             v[r] = ok ? t : mkc((T)0, (T)0);
         }
     }
@@ -334,7 +331,7 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
         else cp_async_wait<0>();
     }
     C* line = sm + c * F::SC;
-    F::template fft<HIN>(v, line, p, tws, MODE == 1);
+    F::template fft<INS == SH_HALF>(v, line, p, tws, MODE == 1);
     if constexpr (MODE == 2) {
         cp_async_wait_all();
         __syncthreads();
@@ -358,8 +355,8 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
         C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
         const int os = F::P * (int)a.out_lstr;
 #pragma unroll
-        for (int r = 0; r < R1; ++r) {
-            if (HOUT ? (r < R1 / 2) : (p + F::P * r < a.nout)) stg(out + r * os, v[r]);
+        for (int r = 0; r < NST; ++r) {
+            if (OUTS != SH_ANY || p + F::P * r < a.nout) out[r * os] = v[r];
         }
     }
 }
@@ -383,7 +380,9 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     const int comp = blockIdx.y;
     const bool valid = row < a.nrows;
     const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
-    const IT* src = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2 + 2 * p;
+    // rows past the end read the array's first elements and drop them (no branch)
+    const IT* src = valid ? reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2 + 2 * p
+                          : reinterpret_cast<const IT*>(a.in);
     C v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
@@ -391,15 +390,13 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
         if (HALF && r >= R1 / 2) {
             v[r] = mkc((T)0, (T)0);
         } else if (HALF) {
-            V d;
-            ldg(reinterpret_cast<const V*>(valid ? src + 2 * F::P * r : reinterpret_cast<const IT*>(a.in)), d);
+            const V d = *reinterpret_cast<const V*>(src + 2 * F::P * r);
             v[r] = valid ? mkc((T)d.x, (T)d.y) : mkc((T)0, (T)0);
         } else {
             const bool two = valid && 2 * j + 1 < a.nin, one = valid && 2 * j + 1 == a.nin;
-            V d;
-            ldg(reinterpret_cast<const V*>(two ? src + 2 * F::P * r : reinterpret_cast<const IT*>(a.in)), d);
-            const IT s1 = one ? src[2 * F::P * r] : (IT)0;
-            v[r] = two ? mkc((T)d.x, (T)d.y) : mkc((T)s1, (T)0);
+            const V d = *reinterpret_cast<const V*>(src + (two ? 2 * F::P * r : 0));
+            const IT s1 = src[one ? 2 * F::P * r : 0];
+            v[r] = two ? mkc((T)d.x, (T)d.y) : (one ? mkc((T)s1, (T)0) : mkc((T)0, (T)0));
         }
     }
     const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
@@ -414,33 +411,26 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     // X[k] = 1/2 (Z_k + conj Z_{LH-k}) - i/2 W_L^k (Z_k - conj Z_{LH-k}),  Z_LH = Z_0
     if constexpr (RowTw<T, LH>::SM) cp_async_wait<0>();
     __syncthreads();
-    const unsigned ls0 = smem_u32(line);
 #pragma unroll
-    for (int r = 0; r < R1; ++r) sts(ls0 + F::sw(p + F::P * r) * (int)sizeof(C), v[r]);
+    for (int r = 0; r < R1; ++r) line[F::sw(p + F::P * r)] = v[r];
     __syncthreads();
     if (valid) {
         C* dst = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2 + p;
-        const unsigned tws0 = smem_u32(wsm + p);
-        const C* twg = reinterpret_cast<const C*>(a.tw) + p;
+        const C* tw = (RowTw<T, LH>::SM ? wsm : reinterpret_cast<const C*>(a.tw)) + p;
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
             const int k = p + F::P * r;
             if (k >= a.nout) continue;
             const C zk = v[r];
-            C zm, wk;
-            lds(ls0 + F::sw((LH - k) & (LH - 1)) * (int)sizeof(C), zm);
-            zm = cconj(zm);
-            if constexpr (RowTw<T, LH>::SM) lds(tws0 + F::P * r * (int)sizeof(C), wk);
-            else wk = __ldg(twg + F::P * r);
+            const C zm = cconj(line[F::sw((LH - k) & (LH - 1))]);
             const C e = cadd(zk, zm);
             const C d = csub(zk, zm);
-            const C w = cmul(wk, d);  // W_L^k (Z_k - conj Z_{LH-k})
-            stg(dst + F::P * r, mkc((T)0.5 * (e.x + w.y), (T)0.5 * (e.y - w.x)));
+            const C w = cmul(tw[F::P * r], d);  // W_L^k (Z_k - conj Z_{LH-k})
+            dst[F::P * r] = mkc((T)0.5 * (e.x + w.y), (T)0.5 * (e.y - w.x));
         }
         if (p == 0 && LH < a.nout) {
-            C z0;
-            lds(ls0, z0);
-            stg(dst + LH, mkc(z0.x - z0.y, (T)0));
+            const C z0 = line[0];
+            dst[LH] = mkc(z0.x - z0.y, (T)0);
         }
     }
 }
@@ -467,42 +457,36 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
         cp_async_commit();
     }
     const C* src = reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
-    // stage the half spectrum X[0..LH] (line positions 0..LH-1, X[LH] kept aside in registers)
-    const unsigned ls0 = smem_u32(line);
+    // stage the half spectrum X[0..LH] (line positions 0..LH-1, X[LH] kept aside in registers);
+    // rows past the end read the array's first element and drop it (no branch)
     const C* srcv = valid ? src : reinterpret_cast<const C*>(a.in);
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
         const int k = p + F::P * r;
-        C t;
-        ldg(srcv + (valid ? k : 0), t);
-        sts(ls0 + F::sw(k) * (int)sizeof(C), valid ? t : mkc((T)0, (T)0));
+        const C t = srcv[valid ? k : 0];
+        line[F::sw(k)] = valid ? t : mkc((T)0, (T)0);
     }
-    C xlh;
-    ldg(srcv + (valid ? LH : 0), xlh);
-    if (!valid) xlh = mkc((T)0, (T)0);
+    const C xl = srcv[valid ? LH : 0];
+    const C xlh = valid ? xl : mkc((T)0, (T)0);
     if constexpr (F::TWS || RowTw<T, LH>::SM) cp_async_wait<0>();
     __syncthreads();
     // Z'_k = A_k + i B_k, A = X_k + conj X_{LH-k}, B = (X_k - conj X_{LH-k}) W_L^{-k};
     // Im X_0 and Im X_LH do not enter a real inverse transform
-    const unsigned tws0 = smem_u32(wsm + p);
-    const C* twg = reinterpret_cast<const C*>(a.tw) + p;
+    const C* tw = (RowTw<T, LH>::SM ? wsm : reinterpret_cast<const C*>(a.tw)) + p;
     C v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
         const int k = p + F::P * r;
-        C xk, xm, wk;
-        lds(ls0 + F::sw(k) * (int)sizeof(C), xk);
-        lds(ls0 + F::sw((LH - k) & (LH - 1)) * (int)sizeof(C), xm);
+        C xk = line[F::sw(k)];
+        C xm = line[F::sw((LH - k) & (LH - 1))];
         if (k == 0) {
             xm = xlh;
             xk.y = (T)0;
             xm.y = (T)0;
         }
         xm = cconj(xm);
-        if constexpr (RowTw<T, LH>::SM) lds(tws0 + F::P * r * (int)sizeof(C), wk);
-        else wk = __ldg(twg + F::P * r);
         const C A = cadd(xk, xm);
-        const C B = cmul(csub(xk, xm), cconj(wk));
+        const C B = cmul(csub(xk, xm), cconj(tw[F::P * r]));
         v[r] = mkc(A.x - B.y, A.y + B.x);
     }
     F::template fft<false>(v, line, p, tws, true);
@@ -512,9 +496,9 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
         for (int r = 0; r < R1; ++r) {
             const int j = p + F::P * r;
             if (HALF) {
-                if (r < R1 / 2) stg(reinterpret_cast<V*>(dst + 2 * F::P * r), V{(OT)v[r].x, (OT)v[r].y});
+                if (r < R1 / 2) *reinterpret_cast<V*>(dst + 2 * F::P * r) = V{(OT)v[r].x, (OT)v[r].y};
             } else {
-                if (2 * j + 1 < a.nout) stg(reinterpret_cast<V*>(dst + 2 * F::P * r), V{(OT)v[r].x, (OT)v[r].y});
+                if (2 * j + 1 < a.nout) *reinterpret_cast<V*>(dst + 2 * F::P * r) = V{(OT)v[r].x, (OT)v[r].y};
                 else if (2 * j < a.nout) dst[2 * F::P * r] = (OT)v[r].x;
             }
         }
@@ -522,34 +506,34 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
 }
 
 // ---------------------------------------------------------------- dispatch
-template <typename T, int L, int R1, int TX, int MODE, bool HALF>
+template <typename T, int L, int R1, int TX, int MODE, int SH>
 static cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, L, R1>;
     const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C) +
                         (MODE == 2 ? (size_t)GStage<L>::N * TX * sizeof(T) : 0);
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(col_dft_kernel<T, L, R1, TX, MODE, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(col_dft_kernel<T, L, R1, TX, MODE, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
         attr = true;
     }
     dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
-    col_dft_kernel<T, L, R1, TX, MODE, HALF><<<grid, TX * F::P, smem, s>>>(a);
+    col_dft_kernel<T, L, R1, TX, MODE, SH><<<grid, TX * F::P, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename T, int MODE, bool HALF>
+template <typename T, int MODE, int SH>
 static cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
     constexpr int TX = sizeof(T) == 4 ? 8 : 4;  // one 64-byte segment of a row per warp access
     switch (L) {
-        case 64: return launch_col_t<T, 64, R1, TX, MODE, HALF>(a, ncomp, s);
-        case 128: return launch_col_t<T, 128, R1, TX, MODE, HALF>(a, ncomp, s);
-        case 256: return launch_col_t<T, 256, R1, TX, MODE, HALF>(a, ncomp, s);
-        case 512: return launch_col_t<T, 512, R1, TX, MODE, HALF>(a, ncomp, s);
-        case 1024: return launch_col_t<T, 1024, R1, TX, MODE, HALF>(a, ncomp, s);
-        case 2048: return launch_col_t<T, 2048, R1, TX / 2, MODE, HALF>(a, ncomp, s);  // keep CTAs at 256 threads
+        case 64: return launch_col_t<T, 64, R1, TX, MODE, SH>(a, ncomp, s);
+        case 128: return launch_col_t<T, 128, R1, TX, MODE, SH>(a, ncomp, s);
+        case 256: return launch_col_t<T, 256, R1, TX, MODE, SH>(a, ncomp, s);
+        case 512: return launch_col_t<T, 512, R1, TX, MODE, SH>(a, ncomp, s);
+        case 1024: return launch_col_t<T, 1024, R1, TX, MODE, SH>(a, ncomp, s);
+        case 2048: return launch_col_t<T, 2048, R1, TX / 2, MODE, SH>(a, ncomp, s);  // keep CTAs at 256 threads
     }
     return cudaErrorInvalidValue;
 }
@@ -562,21 +546,26 @@ int fast_radix1(int f64) { return f64 ? 16 : 32; }
 int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1(f64)); }
 
 template <typename T, int MODE>
-static cudaError_t launch_col_half(bool half, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    return half ? launch_col_mode<T, MODE, true>(L, a, ncomp, s) : launch_col_mode<T, MODE, false>(L, a, ncomp, s);
+static cudaError_t launch_col_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    if (sh == SH_FULL) return launch_col_mode<T, MODE, SH_FULL>(L, a, ncomp, s);
+    if (sh == SH_HALF) return launch_col_mode<T, MODE, SH_HALF>(L, a, ncomp, s);
+    return launch_col_mode<T, MODE, SH_ANY>(L, a, ncomp, s);
 }
 
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    const bool hin = 2 * a.nin == L, hout = 2 * a.nout == L;
-    const bool half = (mode == 0) ? hin : (mode == 1) ? hout : (hin && hout);
+    auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };
+    int sh;
+    if (mode == 0) sh = (a.nout == L) ? shape(a.nin) : SH_ANY;
+    else if (mode == 1) sh = (a.nin == L) ? shape(a.nout) : SH_ANY;
+    else sh = (shape(a.nin) == shape(a.nout)) ? shape(a.nin) : SH_ANY;
     if (f64) {
-        if (mode == 0) return launch_col_half<double, 0>(half, L, a, ncomp, s);
-        if (mode == 1) return launch_col_half<double, 1>(half, L, a, ncomp, s);
-        return launch_col_half<double, 2>(half, L, a, ncomp, s);
+        if (mode == 0) return launch_col_shape<double, 0>(sh, L, a, ncomp, s);
+        if (mode == 1) return launch_col_shape<double, 1>(sh, L, a, ncomp, s);
+        return launch_col_shape<double, 2>(sh, L, a, ncomp, s);
     }
-    if (mode == 0) return launch_col_half<float, 0>(half, L, a, ncomp, s);
-    if (mode == 1) return launch_col_half<float, 1>(half, L, a, ncomp, s);
-    return launch_col_half<float, 2>(half, L, a, ncomp, s);
+    if (mode == 0) return launch_col_shape<float, 0>(sh, L, a, ncomp, s);
+    if (mode == 1) return launch_col_shape<float, 1>(sh, L, a, ncomp, s);
+    return launch_col_shape<float, 2>(sh, L, a, ncomp, s);
 }
 
 template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
