@@ -133,6 +133,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes (read + write) per launch / algorithmic bytes per launch of each pass,
+# from one ncu capture of the same kernels on the 256^3 case
+# (profiles/col_dft_256cube_fp32_full.md, profiles/row_dft_256cube_fp32_full.md);
+# the traffic of a 512^3 launch is this ratio times its algorithmic bytes
+# (traffic grows with the lines processed)
+TRAFFIC_RATIO_256 = {"fused": 583.7 / 606.9, "fwd1": 369.0 / 404.2, "bwd1": 397.7 / 404.2,
+                     "fwd0": 228.8 / 269.1, "bwd0": 228.4 / 269.1}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -365,7 +374,10 @@ def main():
         "fp64": {"value": world * n ** 3 / (ms64 * 1e-3), "ms_per_step": ms64},
         "setup_s": {"fp32": setup32, "fp64": setup64},
         "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (TRAFFIC_RATIO_256[dom["name"]] * dom["bytes"]
+                                 if (n == 512 and args.kernel == "LGF_2" and dom["name"] in TRAFFIC_RATIO_256) else None),
+                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum of the 256^3 launch, scaled by lines",
                      "bytes_per_launch": dom["bytes"], "ms_per_launch": dom_ms,
                      "solve_bytes": tot_bytes, "solve_frac": tot_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
                      "passes": [{"name": p["name"], "ms": p["ms_total"] / max(1, p["calls"]), "bytes": p["bytes"]} for p in stats]},

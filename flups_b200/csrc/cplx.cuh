@@ -22,6 +22,7 @@ template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc(a
 // rounding as the scalar operation); a - b as b * (-1) + a, exact in the product
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 #endif
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
     return mkc(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

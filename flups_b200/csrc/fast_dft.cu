@@ -336,14 +336,11 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
         cp_async_wait_all();
         __syncthreads();
         // k = p + P r; fold(k) = k for r < R1/2, L - k for r >= R1/2 (k = L/2 included)
+        // the stored spectrum already carries the normalisation
         const T* g0 = gs + p * TX + c;
         const T* g1 = gs + (L - p) * TX + c;
-        const T nf = (T)a.normfact;
 #pragma unroll
-        for (int r = 0; r < R1; ++r) {
-            const T gv = (r < R1 / 2 ? g0[r * F::P * TX] : g1[-r * F::P * TX]) * nf;
-            v[r] = mkc(v[r].x * gv, v[r].y * gv);
-        }
+        for (int r = 0; r < R1; ++r) v[r] = cscale(v[r], r < R1 / 2 ? g0[r * F::P * TX] : g1[-r * F::P * TX]);
         // the table plus an offset the compiler cannot see is zero: it cannot
         // merge the second DFT's twiddle loads with the first's, so those stay
         // out of registers during the multiply (the state space stays known)
@@ -523,10 +520,14 @@ static cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+#ifndef FLB_FUSED_TX_F32
+#define FLB_FUSED_TX_F32 8
+#endif
 template <typename T, int MODE, int SH>
 static cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
-    constexpr int TX = sizeof(T) == 4 ? 8 : 4;  // one 64-byte segment of a row per warp access
+    // one 64-byte segment of a row per warp access
+    constexpr int TX = sizeof(T) == 4 ? (MODE == 2 ? FLB_FUSED_TX_F32 : 8) : 4;
     switch (L) {
         case 64: return launch_col_t<T, 64, R1, TX, MODE, SH>(a, ncomp, s);
         case 128: return launch_col_t<T, 128, R1, TX, MODE, SH>(a, ncomp, s);

@@ -435,6 +435,7 @@ __global__ void green_final_kernel(const GreenFinalArgs A) {
             v = g_0unb3spe(A.kind, ksqr, kk[A.ax[0]], kk[A.ax[1]], kk[A.ax[2]], A.hgrid, A.length);
         }
         if (A.reset0 && id == 0) v = 0.0;
+        v *= A.scale;
         const int64_t o = I[0] * A.fold_str[0] + I[1] * A.fold_str[1] + I[2] * A.fold_str[2];
         if (A.out_f64) reinterpret_cast<double*>(A.out)[o] = v;
         else reinterpret_cast<float*>(A.out)[o] = (float)v;

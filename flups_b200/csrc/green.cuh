@@ -58,6 +58,7 @@ struct GreenFinalArgs {
     int ax[3];
     double hgrid, length;
     int reset0;               // set the (0,0,0) mode to zero
+    double scale;             // the solver's normalisation, folded into the stored spectrum
     void* out;
     int out_f64;
 };

@@ -371,7 +371,7 @@ MultSpec Solver::mult_spec(int type) const {
         G.gn[d] = gfold_n[d];
         G.hgrid[d] = h[d];
     }
-    G.normfact = normfact;
+    G.normfact = 1.0;  // already in the stored spectrum (compute_green)
     G.odiff = odiff;
     if (type == ROT) {
         double kabs[3], ko[3], ss[3];
@@ -870,6 +870,9 @@ void Solver::compute_green() {
     F.hgrid = h[0];
     F.length = length;
     F.reset0 = (F.complete || nunb == 0) && (koffset[0] + koffset[1] + koffset[2] < 0.2);
+    // the stored spectrum is normfact * volfact * G (dothemagic's normfact applied
+    // once here instead of per solve)
+    F.scale = normfact;
     F.out = green;
     F.out_f64 = f64;
     check_cuda(launch_green_final(F, stream), "Green finalisation");
