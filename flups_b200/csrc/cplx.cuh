@@ -32,7 +32,7 @@ template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc(a.x, 
 template <typename C> __device__ __forceinline__ C cmul_mi(C a) { return mkc(a.y, -a.x); }
 template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) { return mkc(a.x * s, a.y * s); }
 
-template <typename C> __device__ __forceinline__ void dft2(C* v) {
+template <bool INV = false, typename C> __device__ __forceinline__ void dft2(C* v) {
     C t = v[0];
     v[0] = cadd(t, v[1]);
     v[1] = csub(t, v[1]);
@@ -42,33 +42,56 @@ template <typename C> __device__ __forceinline__ void dft2(C* v) {
 template <typename C> __device__ __forceinline__ C csub_i(C t, C d) { return mkc(t.x + d.y, t.y - d.x); }
 template <typename C> __device__ __forceinline__ C cadd_i(C t, C d) { return mkc(t.x - d.y, t.y + d.x); }
 
-template <typename C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
+// a * conj(w)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C w) {
+    return mkc(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+// a * (+i)
+template <typename C> __device__ __forceinline__ C cmul_pi(C a) { return mkc(-a.y, a.x); }
+
+// INV: the inverse butterfly (conjugate roots of unity), written out so that
+// an inverse transform needs no conjugation of its input and output
+template <bool INV = false, typename C> __device__ __forceinline__ void dft4(C& a0, C& a1, C& a2, C& a3) {
     const C t0 = cadd(a0, a2), t1 = csub(a0, a2);
     const C t2 = cadd(a1, a3), d = csub(a1, a3);
     a0 = cadd(t0, t2);
     a2 = csub(t0, t2);
-    a1 = csub_i(t1, d);  // t1 + (-i) d
-    a3 = cadd_i(t1, d);  // t1 - (-i) d
+    if constexpr (INV) {
+        a1 = cadd_i(t1, d);  // t1 + i d
+        a3 = csub_i(t1, d);
+    } else {
+        a1 = csub_i(t1, d);  // t1 + (-i) d
+        a3 = cadd_i(t1, d);
+    }
 }
-template <typename C> __device__ __forceinline__ void dft4(C* v) { dft4(v[0], v[1], v[2], v[3]); }
+template <bool INV = false, typename C> __device__ __forceinline__ void dft4(C* v) { dft4<INV>(v[0], v[1], v[2], v[3]); }
 
 // sqrt(1/2), cos(pi/8), sin(pi/8)
 #define FLB_R2 0.70710678118654752440
 #define FLB_C8 0.92387953251128675613
 #define FLB_S8 0.38268343236508977173
 
-template <typename C> __device__ __forceinline__ void dft8(C* v) {
+template <bool INV = false, typename C> __device__ __forceinline__ void dft8(C* v) {
     using S = decltype(v[0].x);
     C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
     C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-    dft4(e0, e1, e2, e3);
-    dft4(o0, o1, o2, o3);
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
     const S r2 = (S)FLB_R2;
-    o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);  // * W8^1
-    o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // * W8^3
+    if constexpr (INV) {
+        o1 = mkc((o1.x - o1.y) * r2, (o1.x + o1.y) * r2);   // * conj(W8^1)
+        o3 = mkc(-(o3.x + o3.y) * r2, (o3.x - o3.y) * r2);  // * conj(W8^3)
+    } else {
+        o1 = mkc((o1.x + o1.y) * r2, (o1.y - o1.x) * r2);   // * W8^1
+        o3 = mkc((o3.y - o3.x) * r2, -(o3.x + o3.y) * r2);  // * W8^3
+    }
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
     v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-    v[2] = csub_i(e2, o2); v[6] = cadd_i(e2, o2);       // o2 * W8^2 = -i o2
+    if constexpr (INV) {
+        v[2] = cadd_i(e2, o2); v[6] = csub_i(e2, o2);    // o2 * conj(W8^2) = i o2
+    } else {
+        v[2] = csub_i(e2, o2); v[6] = cadd_i(e2, o2);    // o2 * W8^2 = -i o2
+    }
     v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
@@ -86,21 +109,21 @@ template <typename S> __device__ __forceinline__ void w16(int m, S& c, S& s) {
     }
 }
 
-template <typename C> __device__ __forceinline__ void dft16(C* v) {
+template <bool INV = false, typename C> __device__ __forceinline__ void dft16(C* v) {
     using S = decltype(v[0].x);
     // inner DFT4 over j1 of a[j2 + 4 j1], twiddle W16^{j2 k1}, outer DFT4 over j2
 #pragma unroll
-    for (int j2 = 0; j2 < 4; ++j2) dft4(v[j2], v[j2 + 4], v[j2 + 8], v[j2 + 12]);
+    for (int j2 = 0; j2 < 4; ++j2) dft4<INV>(v[j2], v[j2 + 4], v[j2 + 8], v[j2 + 12]);
 #pragma unroll
     for (int j2 = 1; j2 < 4; ++j2) {
 #pragma unroll
         for (int k1 = 1; k1 < 4; ++k1) {
             if (j2 * k1 == 4) {
-                v[j2 + 4 * k1] = cmul_mi(v[j2 + 4 * k1]);
+                v[j2 + 4 * k1] = INV ? cmul_pi(v[j2 + 4 * k1]) : cmul_mi(v[j2 + 4 * k1]);
             } else {
                 S c, s;
                 w16<S>(j2 * k1, c, s);
-                v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, s));
+                v[j2 + 4 * k1] = cmul(v[j2 + 4 * k1], mkc(c, INV ? -s : s));
             }
         }
     }
@@ -108,7 +131,7 @@ template <typename C> __device__ __forceinline__ void dft16(C* v) {
 #pragma unroll
     for (int k1 = 0; k1 < 4; ++k1) {
         C a0 = v[0 + 4 * k1], a1 = v[1 + 4 * k1], a2 = v[2 + 4 * k1], a3 = v[3 + 4 * k1];
-        dft4(a0, a1, a2, a3);
+        dft4<INV>(a0, a1, a2, a3);
         t[k1 + 0] = a0; t[k1 + 4] = a1; t[k1 + 8] = a2; t[k1 + 12] = a3;
     }
 #pragma unroll
@@ -139,14 +162,14 @@ template <typename S> __device__ __forceinline__ void w32(int m, S& c, S& s) {
 }
 
 // DFT32 as 4 x 8: inner DFT8 over n2 of a[n1 + 4 n2], twiddle W32^{n1 k2}, outer DFT4 over n1
-template <typename C> __device__ __forceinline__ void dft32(C* v) {
+template <bool INV = false, typename C> __device__ __forceinline__ void dft32(C* v) {
     using S = decltype(v[0].x);
 #pragma unroll
     for (int n1 = 0; n1 < 4; ++n1) {
         C a[8];
 #pragma unroll
         for (int n2 = 0; n2 < 8; ++n2) a[n2] = v[n1 + 4 * n2];
-        dft8(a);
+        dft8<INV>(a);
 #pragma unroll
         for (int k2 = 0; k2 < 8; ++k2) v[n1 + 4 * k2] = a[k2];
     }
@@ -155,11 +178,11 @@ template <typename C> __device__ __forceinline__ void dft32(C* v) {
 #pragma unroll
         for (int k2 = 1; k2 < 8; ++k2) {
             if (n1 * k2 == 8) {
-                v[n1 + 4 * k2] = cmul_mi(v[n1 + 4 * k2]);
+                v[n1 + 4 * k2] = INV ? cmul_pi(v[n1 + 4 * k2]) : cmul_mi(v[n1 + 4 * k2]);
             } else {
                 S c, s;
                 w32<S>(n1 * k2, c, s);
-                v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, s));
+                v[n1 + 4 * k2] = cmul(v[n1 + 4 * k2], mkc(c, INV ? -s : s));
             }
         }
     }
@@ -167,7 +190,7 @@ template <typename C> __device__ __forceinline__ void dft32(C* v) {
 #pragma unroll
     for (int k2 = 0; k2 < 8; ++k2) {
         C a0 = v[0 + 4 * k2], a1 = v[1 + 4 * k2], a2 = v[2 + 4 * k2], a3 = v[3 + 4 * k2];
-        dft4(a0, a1, a2, a3);
+        dft4<INV>(a0, a1, a2, a3);
         t[k2 + 0] = a0; t[k2 + 8] = a1; t[k2 + 16] = a2; t[k2 + 24] = a3;
     }
 #pragma unroll

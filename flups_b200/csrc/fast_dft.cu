@@ -29,13 +29,13 @@
 
 namespace flb {
 
-template <int R, typename C>
+template <int R, bool INV = false, typename C>
 __device__ __forceinline__ void dftr(C* v) {
-    if constexpr (R == 2) dft2(v);
-    else if constexpr (R == 4) dft4(v);
-    else if constexpr (R == 8) dft8(v);
-    else if constexpr (R == 16) dft16(v);
-    else if constexpr (R == 32) dft32(v);
+    if constexpr (R == 2) dft2<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 16) dft16<INV>(v);
+    else if constexpr (R == 32) dft32<INV>(v);
 }
 
 // radix-R DFT of v whose upper half is zero
@@ -91,7 +91,7 @@ struct RegFFT {
     __device__ static __forceinline__ int sw(int i) { return i + (i >> 5); }
 
     // Stockham stage with Ns-point sub-transforms done; tws = this stage's table
-    template <int Ns>
+    template <int Ns, bool INV>
     __device__ static __forceinline__ void stages(C* v, C* sm, int p, const C* __restrict__ tws) {
         constexpr int Rs = (L / Ns < R1) ? (L / Ns) : R1;
         constexpr int NB = R1 / Rs;  // butterflies per thread
@@ -114,10 +114,15 @@ struct RegFFT {
             for (int rp = 0; rp < Rs / 2; ++rp) {
                 C w0, w1;
                 TwPair<T, TWS>::ld(tb + 2 * rp * P, w0, w1);
-                if (rp > 0) t[b * Rs + 2 * rp] = cmul(t[b * Rs + 2 * rp], w0);
-                t[b * Rs + 2 * rp + 1] = cmul(t[b * Rs + 2 * rp + 1], w1);
+                if constexpr (INV) {
+                    if (rp > 0) t[b * Rs + 2 * rp] = cmulc(t[b * Rs + 2 * rp], w0);
+                    t[b * Rs + 2 * rp + 1] = cmulc(t[b * Rs + 2 * rp + 1], w1);
+                } else {
+                    if (rp > 0) t[b * Rs + 2 * rp] = cmul(t[b * Rs + 2 * rp], w0);
+                    t[b * Rs + 2 * rp + 1] = cmul(t[b * Rs + 2 * rp + 1], w1);
+                }
             }
-            dftr<Rs>(&t[b * Rs]);
+            dftr<Rs, INV>(&t[b * Rs]);
         }
         if constexpr (Ns * Rs == L) {
 #pragma unroll
@@ -140,20 +145,17 @@ struct RegFFT {
                 }
             }
             __syncthreads();
-            stages<Ns * Rs>(v, sm, p, tws + L);
+            stages<Ns * Rs, INV>(v, sm, p, tws + L);
         }
     }
 
-    // in place on v: forward (or inverse) unnormalised DFT of the line held as
+    // in place on v: forward (INV: inverse) unnormalised DFT of the line held as
     // v[r] = x[p + P r]; ZIN: x is zero from L/2 on (v[r] = 0 for r >= R1/2)
-    template <bool ZIN>
-    __device__ static __forceinline__ void fft(C* v, C* sm, int p, const C* __restrict__ tws, bool inv) {
-        if (inv) {
-#pragma unroll
-            for (int r = 0; r < R1; ++r) v[r] = cconj(v[r]);
-        }
+    template <bool ZIN, bool INV>
+    __device__ static __forceinline__ void fft(C* v, C* sm, int p, const C* __restrict__ tws) {
+        static_assert(!(ZIN && INV), "zero-padded inputs are forward transforms here");
         if constexpr (ZIN) dftz<R1>(v);
-        else dftr<R1>(v);
+        else dftr<R1, INV>(v);
         if constexpr (P > 1) {
             __syncthreads();
             // sw(p R1 + k) = sw(p R1) + k for k < R1 <= 32
@@ -161,11 +163,7 @@ struct RegFFT {
 #pragma unroll
             for (int k = 0; k < R1; ++k) d0[k] = v[k];
             __syncthreads();
-            stages<R1>(v, sm, p, tws);
-        }
-        if (inv) {
-#pragma unroll
-            for (int r = 0; r < R1; ++r) v[r] = cconj(v[r]);
+            stages<R1, INV>(v, sm, p, tws);
         }
     }
 };
@@ -331,7 +329,8 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
         else cp_async_wait<0>();
     }
     C* line = sm + c * F::SC;
-    F::template fft<INS == SH_HALF>(v, line, p, tws, MODE == 1);
+    if constexpr (MODE == 1) F::template fft<false, true>(v, line, p, tws);
+    else F::template fft<INS == SH_HALF, false>(v, line, p, tws);
     if constexpr (MODE == 2) {
         cp_async_wait_all();
         __syncthreads();
@@ -346,7 +345,7 @@ __global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col
         // out of registers during the multiply (the state space stays known)
         int zero = 0;
         asm("" : "+r"(zero));
-        F::template fft<false>(v, line, p, tws + zero, true);
+        F::template fft<false, true>(v, line, p, tws + zero);
     }
     if (valid) {
         C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
@@ -404,7 +403,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     }
     if constexpr (F::TWS) cp_async_wait<RowTw<T, LH>::SM ? 1 : 0>();
     C* line = sm + rr * F::SC;
-    F::template fft<HALF>(v, line, p, tws, false);
+    F::template fft<HALF, false>(v, line, p, tws);
     // X[k] = 1/2 (Z_k + conj Z_{LH-k}) - i/2 W_L^k (Z_k - conj Z_{LH-k}),  Z_LH = Z_0
     if constexpr (RowTw<T, LH>::SM) cp_async_wait<0>();
     __syncthreads();
@@ -486,7 +485,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
         const C B = cmul(csub(xk, xm), cconj(tw[F::P * r]));
         v[r] = mkc(A.x - B.y, A.y + B.x);
     }
-    F::template fft<false>(v, line, p, tws, true);
+    F::template fft<false, true>(v, line, p, tws);
     if (valid) {
         OT* dst = reinterpret_cast<OT*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2 + 2 * p;
 #pragma unroll

@@ -1,5 +1,7 @@
 // FP64 Green's function evaluation and finalisation kernels (see green.cuh).
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <math_constants.h>
 
 #include "green.cuh"
@@ -373,13 +375,16 @@ __device__ __forceinline__ int symid_g(int i, double symstart) {
 }
 
 __global__ void green_eval_kernel(const GreenEvalArgs A) {
-    const int64_t n0 = A.size[0], n1 = A.size[1], n2 = A.size[2];
-    const int64_t total = n0 * n1 * n2;
-    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n0 = A.size[0], n1 = A.size[1];
+    const int64_t c0 = A.canon ? A.csize[0] : A.size[0], c1 = A.canon ? A.csize[1] : A.size[1];
+    const int64_t c2 = A.canon ? A.csize[2] : A.size[2];
+    const int64_t total = c0 * c1 * c2;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         int I[3];
-        I[0] = (int)(id % n0);
-        I[1] = (int)((id / n0) % n1);
-        I[2] = (int)(id / (n0 * n1));
+        I[0] = (int)(t % c0);
+        I[1] = (int)((t / c0) % c1);
+        I[2] = (int)(t / (c0 * c1));
+        const int64_t id = I[0] + n0 * (I[1] + n1 * (int64_t)I[2]);
         int is[3];
         double x[3], kk[3];
         for (int d = 0; d < 3; ++d) {
@@ -417,6 +422,32 @@ __global__ void green_eval_kernel(const GreenEvalArgs A) {
     }
 }
 
+// every index outside the canonical box takes the value of its mirror image
+// |symid| inside the box (3 unbounded directions: the function depends on |is|)
+__global__ void green_mirror_kernel(const GreenEvalArgs A) {
+    const int64_t n0 = A.size[0], n1 = A.size[1], n2 = A.size[2];
+    const int64_t total = n0 * n1 * n2;
+    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += (int64_t)gridDim.x * blockDim.x) {
+        int I[3], S[3];
+        I[0] = (int)(id % n0);
+        I[1] = (int)((id / n0) % n1);
+        I[2] = (int)(id / (n0 * n1));
+        bool inside = true;
+        for (int d = 0; d < 3; ++d) {
+            S[d] = I[d] < A.csize[d] ? I[d] : abs(symid_g(I[d], A.symstart[d]));
+            inside = inside && (I[d] < A.csize[d]);
+        }
+        if (inside) continue;
+        const int64_t src = S[0] + n0 * (S[1] + n1 * (int64_t)S[2]);
+        if (A.cplx) {
+            A.out[2 * id] = A.out[2 * src];
+            A.out[2 * id + 1] = 0.0;
+        } else {
+            A.out[id] = A.out[src];
+        }
+    }
+}
+
 __global__ void green_final_kernel(const GreenFinalArgs A) {
     const int64_t n0 = A.fold_n[0], n1 = A.fold_n[1], n2 = A.fold_n[2];
     const int64_t total = n0 * n1 * n2;
@@ -442,12 +473,30 @@ __global__ void green_final_kernel(const GreenFinalArgs A) {
     }
 }
 
-cudaError_t launch_green_eval(const GreenEvalArgs& A, cudaStream_t s) {
-    const int64_t total = (int64_t)A.size[0] * A.size[1] * A.size[2];
+cudaError_t launch_green_eval(const GreenEvalArgs& Ain, cudaStream_t s) {
+    GreenEvalArgs A = Ain;
+    A.canon = 0;
+    if (A.nunb == 3) {
+        // the canonical box: 0..floor(symstart) along each mirrored direction;
+        // beyond it |symid| falls back inside the box
+        A.canon = 1;
+        for (int d = 0; d < 3; ++d) {
+            int c = A.size[d];
+            if (A.symstart[d] > 0.0) c = std::min(A.size[d], (int)floor(A.symstart[d]) + 1);
+            A.csize[d] = c;
+        }
+    }
+    const int64_t total = A.canon ? (int64_t)A.csize[0] * A.csize[1] * A.csize[2] : (int64_t)A.size[0] * A.size[1] * A.size[2];
     int64_t nb = (total + 255) / 256;
     if (nb > 148 * 64) nb = 148 * 64;
     if (nb < 1) nb = 1;
     green_eval_kernel<<<(unsigned)nb, 256, 0, s>>>(A);
+    if (A.canon) {
+        const int64_t all = (int64_t)A.size[0] * A.size[1] * A.size[2];
+        int64_t nm = (all + 255) / 256;
+        if (nm > 148 * 64) nm = 148 * 64;
+        green_mirror_kernel<<<(unsigned)std::max<int64_t>(nm, 1), 256, 0, s>>>(A);
+    }
     return cudaGetLastError();
 }
 

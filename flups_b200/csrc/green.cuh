@@ -41,6 +41,11 @@ struct GreenEvalArgs {
     int nfar;
     double far_log;
     double* out;
+    // canonical box: with 3 unbounded directions the function depends on |is|
+    // only, so only indices up to symstart are evaluated and a second kernel
+    // copies them to their mirror images
+    int canon;
+    int csize[3];
 };
 
 struct GreenFinalArgs {
