@@ -50,7 +50,7 @@ def sources():
 
 def build(verbose=False, extra=()):
     gen_farfield()
-    objs = []
+    objs, jobs = [], []
     for src in sources():
         obj = BUILD / (src.stem + ".o")
         deps = [src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + \
@@ -63,8 +63,14 @@ def build(verbose=False, extra=()):
             cmd += ["-c", str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        for r in ex.map(lambda c: subprocess.run(c), jobs):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-ldl"]
     subprocess.run(cmd, check=True)

@@ -235,6 +235,12 @@ void flups_set_precision(Solver* s, int bits) {
 int flups_get_precision(Solver* s) { return s->precision; }
 void flups_set_async(Solver* s, int async) { s->async = async != 0; }
 void flups_b200_set_fast_kernels(Solver* s, int on) { s->use_fast = on != 0; }
+void flups_b200_set_autotune(Solver* s, int on) { s->autotune = on != 0; }
+void flups_b200_set_col_tile(Solver* s, int tile) { s->force_tile = (tile == 1 || tile == 2) ? tile : 0; }
+int flups_solve_graph(Solver* s, double* field, double* rhs, int nbatch, int type) {
+    if (!s) return -1;
+    return s->solve_graph(field, rhs, type, nbatch);
+}
 int flups_get_last_error(Solver* s) { return s->last_error; }
 size_t flups_get_device_bytes(Solver* s, int nbatch) { return s->device_bytes(nbatch); }
 

@@ -1,542 +1,9 @@
-// Register-resident power-of-two DFT passes for the DFT directions of the
-// solve (PERPER and UNBUNB plans, FFTW_plan_dim.cpp:365-451 / :670-716).
-//
-// A line of length L is owned by P = L / R1 threads; thread p holds
-// x[p + P r] for r < R1 in registers.  Stage 1 is a radix-R1 DFT in
-// registers; every later Stockham stage exchanges once through shared
-// memory (one padding element per 32 keeps the accesses of a half-warp on
-// distinct banks) and ends with thread p holding X[p + P r]: the same
-// distribution as the input, so the inverse transform of the fused pass
-// starts from registers and the Green's multiply happens in between without
-// touching the line in shared memory.
-//
-// Instruction economy (the passes run close to the issue limit of the SM):
-// the twiddles of a later stage come from a per-stage table laid out in the
-// order the threads consume them (two per 16-byte load, no index arithmetic);
-// shared-memory and global addresses are a per-thread base plus compile-time
-// offsets; a line zero-padded to twice its length skips the zero half in the
-// first butterflies, and outputs that are truncated are never computed.
-//
-// Column passes (y or z): a CTA owns TX consecutive x columns; lanes are
-// x-fastest so every global access of a warp reads TX consecutive complex
-// values of a few rows.  Row passes (x): r2c / c2r of real rows through a
-// complex DFT of half length (z_j = x_2j + i x_2j+1).
-#include <cuda_runtime.h>
-
-#include "cplx.cuh"
-#include "fast_dft.h"
-#include "pass_desc.h"
+// Dispatch of the register-resident DFT passes (kernels in fast_dft_impl.cuh,
+// instantiated per precision and mode in fast_col_*.cu and fast_row.cu so
+// that the units compile in parallel).
+#include "fast_dft_impl.cuh"
 
 namespace flb {
-
-template <int R, bool INV = false, typename C>
-__device__ __forceinline__ void dftr(C* v) {
-    if constexpr (R == 2) dft2<INV>(v);
-    else if constexpr (R == 4) dft4<INV>(v);
-    else if constexpr (R == 8) dft8<INV>(v);
-    else if constexpr (R == 16) dft16<INV>(v);
-    else if constexpr (R == 32) dft32<INV>(v);
-}
-
-// radix-R DFT of v whose upper half is zero
-template <int R, typename C>
-__device__ __forceinline__ void dftz(C* v) {
-    if constexpr (R == 2) dft2z(v);
-    else if constexpr (R == 4) dft4z(v);
-    else if constexpr (R == 8) dft8z(v);
-    else if constexpr (R == 16) dft16z(v);
-    else if constexpr (R == 32) dft32z(v);
-}
-
-// two consecutive complex twiddles of a stage table, from shared memory
-// (SM) or through the read-only data path
-template <typename T, bool SM> struct TwPair;
-template <bool SM> struct TwPair<float, SM> {
-    __device__ static __forceinline__ void ld(const float2* p, float2& a, float2& b) {
-        const float4 q = SM ? *reinterpret_cast<const float4*>(p) : __ldg(reinterpret_cast<const float4*>(p));
-        a = make_float2(q.x, q.y);
-        b = make_float2(q.z, q.w);
-    }
-};
-template <bool SM> struct TwPair<double, SM> {
-    __device__ static __forceinline__ void ld(const double2* p, double2& a, double2& b) {
-        a = SM ? p[0] : __ldg(p);
-        b = SM ? p[1] : __ldg(p + 1);
-    }
-};
-
-// complex entries of the later-stage table of an n-point DFT with first radix r1
-__host__ __device__ constexpr int stage_table_entries(int n, int r1) {
-    int stages = 0;
-    for (int Ns = r1; Ns < n; Ns *= (n / Ns < r1) ? n / Ns : r1) ++stages;
-    return stages * n;
-}
-
-// ROWS: the lines of a CTA are thread-index-slow (row passes: p fastest),
-// else thread-index-fast (column passes: the TX columns fastest).
-template <typename T, int L, int R1, bool ROWS = false>
-struct RegFFT {
-    using C = typename CT<T>::C;
-    static constexpr int P = L / R1;
-    // the later-stage table is staged in shared memory when it is small
-    // (FP32 lines up to 1024: one later stage, at most 8 KB)
-    static constexpr int TWN = stage_table_entries(L, R1);
-    static constexpr bool TWS = TWN > 0 && TWN * (int)sizeof(C) <= 8192;
-    static constexpr int TW_SMEM = TWS ? TWN : 0;  // complex entries of shared memory for the table
-    // line stride in shared memory (complex elements): the swizzled length rounded
-    // to 16, plus an offset that puts the lines met by one half-warp on distinct
-    // banks: a column CTA has lanes c = 0..TX-1 on TX lines (offset 2 per line,
-    // the lane's p adds 0 or 1); a row CTA has P lanes per line (offset P).
-    static constexpr int SC = ((L + L / 32 + 15) / 16) * 16 + (ROWS ? (P % 16) : 2);
-    __device__ static __forceinline__ int sw(int i) { return i + (i >> 5); }
-
-    // Stockham stage with Ns-point sub-transforms done; tws = this stage's table
-    template <int Ns, bool INV>
-    __device__ static __forceinline__ void stages(C* v, C* sm, int p, const C* __restrict__ tws) {
-        constexpr int Rs = (L / Ns < R1) ? (L / Ns) : R1;
-        constexpr int NB = R1 / Rs;  // butterflies per thread
-        constexpr int MR = L / Rs;
-        C t[R1];
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            const int j = p + P * b;
-            if constexpr (MR % 32 == 0) {
-                // sw(j + r MR) = sw(j) + r (MR + MR/32) when MR is a multiple of 32
-                const C* s0 = sm + sw(j);
-#pragma unroll
-                for (int r = 0; r < Rs; ++r) t[b * Rs + r] = s0[r * (MR + MR / 32)];
-            } else {
-#pragma unroll
-                for (int r = 0; r < Rs; ++r) t[b * Rs + r] = sm[sw(j + r * MR)];
-            }
-            const C* tb = tws + 2 * (b * (Rs / 2) * P + p);
-#pragma unroll
-            for (int rp = 0; rp < Rs / 2; ++rp) {
-                C w0, w1;
-                TwPair<T, TWS>::ld(tb + 2 * rp * P, w0, w1);
-                if constexpr (INV) {
-                    if (rp > 0) t[b * Rs + 2 * rp] = cmulc(t[b * Rs + 2 * rp], w0);
-                    t[b * Rs + 2 * rp + 1] = cmulc(t[b * Rs + 2 * rp + 1], w1);
-                } else {
-                    if (rp > 0) t[b * Rs + 2 * rp] = cmul(t[b * Rs + 2 * rp], w0);
-                    t[b * Rs + 2 * rp + 1] = cmul(t[b * Rs + 2 * rp + 1], w1);
-                }
-            }
-            dftr<Rs, INV>(&t[b * Rs]);
-        }
-        if constexpr (Ns * Rs == L) {
-#pragma unroll
-            for (int b = 0; b < NB; ++b)
-#pragma unroll
-                for (int r = 0; r < Rs; ++r) v[b + NB * r] = t[b * Rs + r];
-        } else {
-            __syncthreads();
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const int j = p + P * b;
-                const int base = (j / Ns) * Ns * Rs + (j % Ns);
-                if constexpr (Ns % 32 == 0) {
-                    C* d0 = sm + sw(base);
-#pragma unroll
-                    for (int r = 0; r < Rs; ++r) d0[r * (Ns + Ns / 32)] = t[b * Rs + r];
-                } else {
-#pragma unroll
-                    for (int r = 0; r < Rs; ++r) sm[sw(base + r * Ns)] = t[b * Rs + r];
-                }
-            }
-            __syncthreads();
-            stages<Ns * Rs, INV>(v, sm, p, tws + L);
-        }
-    }
-
-    // in place on v: forward (INV: inverse) unnormalised DFT of the line held as
-    // v[r] = x[p + P r]; ZIN: x is zero from L/2 on (v[r] = 0 for r >= R1/2)
-    template <bool ZIN, bool INV>
-    __device__ static __forceinline__ void fft(C* v, C* sm, int p, const C* __restrict__ tws) {
-        static_assert(!(ZIN && INV), "zero-padded inputs are forward transforms here");
-        if constexpr (ZIN) dftz<R1>(v);
-        else dftr<R1, INV>(v);
-        if constexpr (P > 1) {
-            __syncthreads();
-            // sw(p R1 + k) = sw(p R1) + k for k < R1 <= 32
-            C* d0 = sm + sw(p * R1);
-#pragma unroll
-            for (int k = 0; k < R1; ++k) d0[k] = v[k];
-            __syncthreads();
-            stages<R1, INV>(v, sm, p, tws);
-        }
-    }
-};
-
-__device__ __forceinline__ int fold_idx(int i, int M) { return (M > 0 && 2 * i > M) ? M - i : i; }
-
-// asynchronous global -> shared copies (LDGSTS): the stage twiddles and the
-// folded Green's values of a fused pass arrive while the line loads are in
-// flight and the first butterflies run
-template <int B>
-__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    if constexpr (B == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem_src), "n"(B) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// the stage table of F into shared memory at dst (one commit group); returns
-// the table to use (dst, or the global table when F keeps it in global memory)
-template <typename F>
-__device__ __forceinline__ const typename F::C* stage_twiddles(const void* gtab, typename F::C* dst) {
-    using C = typename F::C;
-    if constexpr (F::TWS) {
-        constexpr int CHUNKS = F::TWN * (int)sizeof(C) / 16;
-        const char* src = reinterpret_cast<const char*>(gtab);
-        char* d = reinterpret_cast<char*>(dst);
-        for (int e = threadIdx.x; e < CHUNKS; e += blockDim.x) cp_async<16>(d + 16 * e, src + 16 * e);
-        cp_async_commit();
-        return dst;
-    } else {
-        return reinterpret_cast<const C*>(gtab);
-    }
-}
-
-// the first n entries of a global table into shared memory at dst (no commit)
-template <typename C, int n>
-__device__ __forceinline__ void stage_table_part(const void* gtab, C* dst) {
-    constexpr int CHUNKS = n * (int)sizeof(C) / 16;
-    const char* src = reinterpret_cast<const char*>(gtab);
-    char* d = reinterpret_cast<char*>(dst);
-    for (int e = threadIdx.x; e < CHUNKS; e += blockDim.x) cp_async<16>(d + 16 * e, src + 16 * e);
-}
-
-// row passes keep W_L^k, k < Lh (the split of the real transform), in shared
-// memory when it is small
-template <typename T, int LH>
-struct RowTw {
-    using C = typename CT<T>::C;
-    static constexpr bool SM = LH * (int)sizeof(C) <= 8192;
-    static constexpr int N = SM ? LH : 0;
-};
-
-// folded Green's values of a fused CTA: line index j = 0..L/2 (the fold of
-// k and L-k), TX columns x-fastest: gs[j * TX + c]
-template <int L>
-struct GStage {
-    static constexpr int N = L / 2 + 1;
-};
-
-// Fused passes visit the outer index in mirror pairs (0, 1, M-1, 2, M-2, ...,
-// M/2) when the Green's function is folded along it, so the folded Green slab
-// read for o is read again for M-o while it is still in L2.
-__device__ __forceinline__ int mirror_order(int by, int nouter, int fold) {
-    if (fold != nouter || fold < 4) return by;
-    if (by == 0) return 0;
-    if (by == nouter - 1) return nouter / 2;
-    const int m = (by + 1) >> 1;
-    return (by & 1) ? m : nouter - m;
-}
-
-template <typename T, int L, int TX>
-__device__ __forceinline__ void stage_green(const ColArgs& a, T* gs, int o) {
-    constexpr int N = GStage<L>::N;
-    const T* g = reinterpret_cast<const T*>(a.green) + (int64_t)fold_idx(o, a.f_outer) * a.g_outer;
-    const int gl = (int)a.g_line;
-    const int x0 = blockIdx.x * TX;
-    constexpr int PER = 16 / (int)sizeof(T);  // values per 16-byte copy
-    if constexpr (TX % PER == 0) {
-        // Green rows are padded to 128 bytes and x0 is a multiple of TX, so the
-        // TX values of a row are one or two aligned 16-byte pieces inside the row
-        if (a.f_x == 0 && a.g_x == 1 && (reinterpret_cast<uintptr_t>(a.green) & 15) == 0) {
-            constexpr int CH = TX / PER;
-            for (int e = threadIdx.x; e < N * CH; e += blockDim.x) {
-                const int j = e / CH, ch = e % CH;
-                cp_async<16>(gs + j * TX + ch * PER, g + x0 + ch * PER + j * gl);
-            }
-            cp_async_commit();
-            return;
-        }
-    }
-    for (int e = threadIdx.x; e < N * TX; e += blockDim.x) {
-        const int j = e / TX, cc = e % TX, xx = x0 + cc;
-        if (xx < a.nx) cp_async<sizeof(T)>(gs + e, g + (int64_t)fold_idx(xx, a.f_x) * a.g_x + j * gl);
-        else gs[e] = (T)0;
-    }
-    cp_async_commit();
-}
-
-// resident threads per SM the register budget is sized for (2 CTAs of 256
-// threads): the passes are bound by memory and issue, and two resident
-// CTAs overlap one CTA's loads with the other's arithmetic
-#ifndef FLB_COL_THREADS_PER_SM
-#define FLB_COL_THREADS_PER_SM 512
-#endif
-template <int THREADS>
-struct Occ {
-    static constexpr int want = FLB_COL_THREADS_PER_SM / (THREADS < 64 ? 64 : THREADS);
-    static constexpr int blocks = want < 1 ? 1 : want;
-};
-
-// ---------------------------------------------------------------- columns
-// Extent of the loaded / stored part of a line, known at compile time:
-enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
-// MODE 0: forward DFT (SH: loaded part; SH != ANY also means all L stored),
-//      1: inverse DFT (SH: stored part; SH != ANY also means all L loaded),
-//      2: forward, Green multiply, inverse (SH: loaded and stored part).
-// The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
-template <typename T, int L, int R1, int TX, int MODE, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col_dft_kernel(const ColArgs a) {
-    using F = RegFFT<T, L, R1>;
-    using C = typename CT<T>::C;
-    constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
-    constexpr int OUTS = (MODE == 0) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
-    constexpr int NLD = (INS == SH_HALF) ? R1 / 2 : R1;  // registers loaded
-    constexpr int NST = (OUTS == SH_HALF) ? R1 / 2 : R1;  // registers stored
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    const int c = threadIdx.x % TX, p = threadIdx.x / TX;
-    const int x = blockIdx.x * TX + c;
-    const int o = (MODE == 2) ? mirror_order(blockIdx.y, a.nouter, a.f_outer) : (int)blockIdx.y;
-    const int comp = blockIdx.z;
-    const bool valid = x < a.nx;
-    // shared memory: TX lines of the exchange, the stage table, the Green's values
-    const C* tws = stage_twiddles<F>(a.tws, sm + TX * F::SC);
-    T* gs = reinterpret_cast<T*>(sm + TX * F::SC + F::TW_SMEM);
-    if constexpr (MODE == 2) stage_green<T, L, TX>(a, gs, o);
-    // lanes outside the array read its first element and drop it (no branch)
-    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
-                        : reinterpret_cast<const C*>(a.in);
-    const int ls = valid ? F::P * (int)a.in_lstr : 0;
-    C v[R1];
-#pragma unroll
-    for (int r = 0; r < R1; ++r) {
-        if (r >= NLD) {
-            v[r] = mkc((T)0, (T)0);
-        } else if constexpr (INS != SH_ANY) {
-            const C t = in[r * ls];
-            v[r] = valid ? t : mkc((T)0, (T)0);
-        } else {
-            const bool ok = valid && p + F::P * r < a.nin;
-            const C t = in[ok ? r * ls : 0];
-            v[r] = ok ? t : mkc((T)0, (T)0);
-        }
-    }
-    // the table's copies are complete before the first exchange's barrier
-    if constexpr (F::TWS) {
-        if constexpr (MODE == 2) cp_async_wait<1>();
-        else cp_async_wait<0>();
-    }
-    C* line = sm + c * F::SC;
-    if constexpr (MODE == 1) F::template fft<false, true>(v, line, p, tws);
-    else F::template fft<INS == SH_HALF, false>(v, line, p, tws);
-    if constexpr (MODE == 2) {
-        cp_async_wait_all();
-        __syncthreads();
-        // k = p + P r; fold(k) = k for r < R1/2, L - k for r >= R1/2 (k = L/2 included)
-        // the stored spectrum already carries the normalisation
-        const T* g0 = gs + p * TX + c;
-        const T* g1 = gs + (L - p) * TX + c;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) v[r] = cscale(v[r], r < R1 / 2 ? g0[r * F::P * TX] : g1[-r * F::P * TX]);
-        // the table plus an offset the compiler cannot see is zero: it cannot
-        // merge the second DFT's twiddle loads with the first's, so those stay
-        // out of registers during the multiply (the state space stays known)
-        int zero = 0;
-        asm("" : "+r"(zero));
-        F::template fft<false, true>(v, line, p, tws + zero);
-    }
-    if (valid) {
-        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
-        const int os = F::P * (int)a.out_lstr;
-#pragma unroll
-        for (int r = 0; r < NST; ++r) {
-            if (OUTS != SH_ANY || p + F::P * r < a.nout) out[r * os] = v[r];
-        }
-    }
-}
-
-// ---------------------------------------------------------------- rows: r2c
-template <typename IT> struct Vec2;
-template <> struct Vec2<float> { using V = float2; };
-template <> struct Vec2<double> { using V = double2; };
-
-// IT: type of the real input (the user's double array, or the working precision);
-// HALF: nin = Lh (the row is zero-padded to twice its length)
-template <typename T, typename IT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_r2c_kernel(const RowArgs a) {
-    using F = RegFFT<T, LH, R1, true>;
-    using C = typename CT<T>::C;
-    using V = typename Vec2<IT>::V;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    const int p = threadIdx.x % F::P, rr = threadIdx.x / F::P;
-    const int row = blockIdx.x * TR + rr;
-    const int comp = blockIdx.y;
-    const bool valid = row < a.nrows;
-    const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
-    // rows past the end read the array's first elements and drop them (no branch)
-    const IT* src = valid ? reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2 + 2 * p
-                          : reinterpret_cast<const IT*>(a.in);
-    C v[R1];
-#pragma unroll
-    for (int r = 0; r < R1; ++r) {
-        const int j = p + F::P * r;
-        if (HALF && r >= R1 / 2) {
-            v[r] = mkc((T)0, (T)0);
-        } else if (HALF) {
-            const V d = *reinterpret_cast<const V*>(src + 2 * F::P * r);
-            v[r] = valid ? mkc((T)d.x, (T)d.y) : mkc((T)0, (T)0);
-        } else {
-            const bool two = valid && 2 * j + 1 < a.nin, one = valid && 2 * j + 1 == a.nin;
-            const V d = *reinterpret_cast<const V*>(src + (two ? 2 * F::P * r : 0));
-            const IT s1 = src[one ? 2 * F::P * r : 0];
-            v[r] = two ? mkc((T)d.x, (T)d.y) : (one ? mkc((T)s1, (T)0) : mkc((T)0, (T)0));
-        }
-    }
-    const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
-    C* wsm = sm + TR * F::SC + F::TW_SMEM;
-    if constexpr (RowTw<T, LH>::SM) {
-        stage_table_part<C, LH>(a.tw, wsm);
-        cp_async_commit();
-    }
-    if constexpr (F::TWS) cp_async_wait<RowTw<T, LH>::SM ? 1 : 0>();
-    C* line = sm + rr * F::SC;
-    F::template fft<HALF, false>(v, line, p, tws);
-    // X[k] = 1/2 (Z_k + conj Z_{LH-k}) - i/2 W_L^k (Z_k - conj Z_{LH-k}),  Z_LH = Z_0
-    if constexpr (RowTw<T, LH>::SM) cp_async_wait<0>();
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R1; ++r) line[F::sw(p + F::P * r)] = v[r];
-    __syncthreads();
-    if (valid) {
-        C* dst = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2 + p;
-        const C* tw = (RowTw<T, LH>::SM ? wsm : reinterpret_cast<const C*>(a.tw)) + p;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) {
-            const int k = p + F::P * r;
-            if (k >= a.nout) continue;
-            const C zk = v[r];
-            const C zm = cconj(line[F::sw((LH - k) & (LH - 1))]);
-            const C e = cadd(zk, zm);
-            const C d = csub(zk, zm);
-            const C w = cmul(tw[F::P * r], d);  // W_L^k (Z_k - conj Z_{LH-k})
-            dst[F::P * r] = mkc((T)0.5 * (e.x + w.y), (T)0.5 * (e.y - w.x));
-        }
-        if (p == 0 && LH < a.nout) {
-            const C z0 = line[0];
-            dst[LH] = mkc(z0.x - z0.y, (T)0);
-        }
-    }
-}
-
-// ---------------------------------------------------------------- rows: c2r
-// OT: type of the real output; HALF: nout = Lh (the row is truncated to half)
-template <typename T, typename OT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_c2r_kernel(const RowArgs a) {
-    using F = RegFFT<T, LH, R1, true>;
-    using C = typename CT<T>::C;
-    using V = typename Vec2<OT>::V;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    const int p = threadIdx.x % F::P, rr = threadIdx.x / F::P;
-    const int row = blockIdx.x * TR + rr;
-    const int comp = blockIdx.y;
-    const bool valid = row < a.nrows;
-    const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
-    C* line = sm + rr * F::SC;
-    const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
-    C* wsm = sm + TR * F::SC + F::TW_SMEM;
-    if constexpr (RowTw<T, LH>::SM) {
-        stage_table_part<C, LH>(a.tw, wsm);
-        cp_async_commit();
-    }
-    const C* src = reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
-    // stage the half spectrum X[0..LH] (line positions 0..LH-1, X[LH] kept aside in registers);
-    // rows past the end read the array's first element and drop it (no branch)
-    const C* srcv = valid ? src : reinterpret_cast<const C*>(a.in);
-#pragma unroll
-    for (int r = 0; r < R1; ++r) {
-        const int k = p + F::P * r;
-        const C t = srcv[valid ? k : 0];
-        line[F::sw(k)] = valid ? t : mkc((T)0, (T)0);
-    }
-    const C xl = srcv[valid ? LH : 0];
-    const C xlh = valid ? xl : mkc((T)0, (T)0);
-    if constexpr (F::TWS || RowTw<T, LH>::SM) cp_async_wait<0>();
-    __syncthreads();
-    // Z'_k = A_k + i B_k, A = X_k + conj X_{LH-k}, B = (X_k - conj X_{LH-k}) W_L^{-k};
-    // Im X_0 and Im X_LH do not enter a real inverse transform
-    const C* tw = (RowTw<T, LH>::SM ? wsm : reinterpret_cast<const C*>(a.tw)) + p;
-    C v[R1];
-#pragma unroll
-    for (int r = 0; r < R1; ++r) {
-        const int k = p + F::P * r;
-        C xk = line[F::sw(k)];
-        C xm = line[F::sw((LH - k) & (LH - 1))];
-        if (k == 0) {
-            xm = xlh;
-            xk.y = (T)0;
-            xm.y = (T)0;
-        }
-        xm = cconj(xm);
-        const C A = cadd(xk, xm);
-        const C B = cmul(csub(xk, xm), cconj(tw[F::P * r]));
-        v[r] = mkc(A.x - B.y, A.y + B.x);
-    }
-    F::template fft<false, true>(v, line, p, tws);
-    if (valid) {
-        OT* dst = reinterpret_cast<OT*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2 + 2 * p;
-#pragma unroll
-        for (int r = 0; r < R1; ++r) {
-            const int j = p + F::P * r;
-            if (HALF) {
-                if (r < R1 / 2) *reinterpret_cast<V*>(dst + 2 * F::P * r) = V{(OT)v[r].x, (OT)v[r].y};
-            } else {
-                if (2 * j + 1 < a.nout) *reinterpret_cast<V*>(dst + 2 * F::P * r) = V{(OT)v[r].x, (OT)v[r].y};
-                else if (2 * j < a.nout) dst[2 * F::P * r] = (OT)v[r].x;
-            }
-        }
-    }
-}
-
-// ---------------------------------------------------------------- dispatch
-template <typename T, int L, int R1, int TX, int MODE, int SH>
-static cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, L, R1>;
-    const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C) +
-                        (MODE == 2 ? (size_t)GStage<L>::N * TX * sizeof(T) : 0);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(col_dft_kernel<T, L, R1, TX, MODE, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
-    col_dft_kernel<T, L, R1, TX, MODE, SH><<<grid, TX * F::P, smem, s>>>(a);
-    return cudaGetLastError();
-}
-
-#ifndef FLB_FUSED_TX_F32
-#define FLB_FUSED_TX_F32 8
-#endif
-template <typename T, int MODE, int SH>
-static cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
-    // one 64-byte segment of a row per warp access
-    constexpr int TX = sizeof(T) == 4 ? (MODE == 2 ? FLB_FUSED_TX_F32 : 8) : 4;
-    switch (L) {
-        case 64: return launch_col_t<T, 64, R1, TX, MODE, SH>(a, ncomp, s);
-        case 128: return launch_col_t<T, 128, R1, TX, MODE, SH>(a, ncomp, s);
-        case 256: return launch_col_t<T, 256, R1, TX, MODE, SH>(a, ncomp, s);
-        case 512: return launch_col_t<T, 512, R1, TX, MODE, SH>(a, ncomp, s);
-        case 1024: return launch_col_t<T, 1024, R1, TX, MODE, SH>(a, ncomp, s);
-        case 2048: return launch_col_t<T, 2048, R1, TX / 2, MODE, SH>(a, ncomp, s);  // keep CTAs at 256 threads
-    }
-    return cudaErrorInvalidValue;
-}
 
 bool fast_col_supported(int L) { return L == 64 || L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048; }
 bool fast_row_supported(int L) { return L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048 || L == 4096; }
@@ -545,81 +12,22 @@ int fast_radix1(int f64) { return f64 ? 16 : 32; }
 
 int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1(f64)); }
 
-template <typename T, int MODE>
-static cudaError_t launch_col_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    if (sh == SH_FULL) return launch_col_mode<T, MODE, SH_FULL>(L, a, ncomp, s);
-    if (sh == SH_HALF) return launch_col_mode<T, MODE, SH_HALF>(L, a, ncomp, s);
-    return launch_col_mode<T, MODE, SH_ANY>(L, a, ncomp, s);
-}
-
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };
     int sh;
     if (mode == 0) sh = (a.nout == L) ? shape(a.nin) : SH_ANY;
     else if (mode == 1) sh = (a.nin == L) ? shape(a.nout) : SH_ANY;
     else sh = (shape(a.nin) == shape(a.nout)) ? shape(a.nin) : SH_ANY;
-    if (f64) {
-        if (mode == 0) return launch_col_shape<double, 0>(sh, L, a, ncomp, s);
-        if (mode == 1) return launch_col_shape<double, 1>(sh, L, a, ncomp, s);
-        return launch_col_shape<double, 2>(sh, L, a, ncomp, s);
-    }
-    if (mode == 0) return launch_col_shape<float, 0>(sh, L, a, ncomp, s);
-    if (mode == 1) return launch_col_shape<float, 1>(sh, L, a, ncomp, s);
-    return launch_col_shape<float, 2>(sh, L, a, ncomp, s);
+    if (f64) return (mode == 2) ? launch_col_f64_m2(sh, L, a, ncomp, s) : launch_col_f64_m01(mode, sh, L, a, ncomp, s);
+    if (mode == 2) return launch_col_f32_m2(sh, L, a, ncomp, s);
+    return launch_col_f32_m01(mode, sh, L, a, ncomp, s);
 }
 
-template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
-static cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, LH, R1, true>;
-    constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
-    const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + RowTw<T, LH>::N) * sizeof(typename CT<T>::C);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e;
-        if constexpr (C2R)
-            e = cudaFuncSetAttribute(row_c2r_kernel<T, XT, LH, R1, TR, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        else
-            e = cudaFuncSetAttribute(row_r2c_kernel<T, XT, LH, R1, TR, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    dim3 grid((a.nrows + TR - 1) / TR, ncomp);
-    if constexpr (C2R) row_c2r_kernel<T, XT, LH, R1, TR, HALF><<<grid, TR * F::P, smem, s>>>(a);
-    else row_r2c_kernel<T, XT, LH, R1, TR, HALF><<<grid, TR * F::P, smem, s>>>(a);
-    return cudaGetLastError();
-}
-
-template <typename T, typename XT, bool C2R, bool HALF>
-static cudaError_t launch_row_len(int L, const RowArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
-    switch (L) {
-        case 128: return launch_row_t<T, XT, 64, R1, C2R, HALF>(a, ncomp, s);
-        case 256: return launch_row_t<T, XT, 128, R1, C2R, HALF>(a, ncomp, s);
-        case 512: return launch_row_t<T, XT, 256, R1, C2R, HALF>(a, ncomp, s);
-        case 1024: return launch_row_t<T, XT, 512, R1, C2R, HALF>(a, ncomp, s);
-        case 2048: return launch_row_t<T, XT, 1024, R1, C2R, HALF>(a, ncomp, s);
-        case 4096: return launch_row_t<T, XT, 2048, R1, C2R, HALF>(a, ncomp, s);
-    }
-    return cudaErrorInvalidValue;
-}
-
-template <typename T, typename XT, bool C2R>
-static cudaError_t launch_row_half(bool half, int L, const RowArgs& a, int ncomp, cudaStream_t s) {
-    return half ? launch_row_len<T, XT, C2R, true>(L, a, ncomp, s) : launch_row_len<T, XT, C2R, false>(L, a, ncomp, s);
-}
-
-// XT: the real side's type (r2c input / c2r output): the user's doubles or the working precision
+// the real side (r2c input / c2r output) is the user's doubles or the working precision
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s) {
-    if (f64) {
-        if (c2r) return launch_row_half<double, double, true>(2 * a.nout == L, L, a, ncomp, s);
-        return launch_row_half<double, double, false>(2 * a.nin == L, L, a, ncomp, s);
-    }
-    if (c2r) {
-        if (a.out_f64) return launch_row_half<float, double, true>(2 * a.nout == L, L, a, ncomp, s);
-        return launch_row_half<float, float, true>(2 * a.nout == L, L, a, ncomp, s);
-    }
-    if (a.in_f64) return launch_row_half<float, double, false>(2 * a.nin == L, L, a, ncomp, s);
-    return launch_row_half<float, float, false>(2 * a.nin == L, L, a, ncomp, s);
+    const bool half = c2r ? (2 * a.nout == L) : (2 * a.nin == L);
+    const int xt64 = c2r ? a.out_f64 : a.in_f64;
+    return launch_row_units(f64, c2r, xt64, half, L, a, ncomp, s);
 }
 
 }  // namespace flb

@@ -20,7 +20,10 @@ struct ColArgs {
     int64_t g_x, g_line, g_outer;          // folded Green strides
     int f_x, f_line, f_outer;              // fold lengths (0 = none)
     double normfact;
+    int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
 };
+
+enum { COL_TILE_DEFAULT = 0, COL_TILE_256 = 1, COL_TILE_128 = 2 };
 
 struct RowArgs {
     const void* in;

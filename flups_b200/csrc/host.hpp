@@ -152,6 +152,31 @@ struct Solver {
     // ---------------------------------------------------------------- per-pass timing
     bool timing = false;
     int pass_idx = 0;
+    // CTA-tile autotuning of the column passes: per pass signature, the tile
+    // that ran fastest on this GPU (timed once per signature, before the solve)
+    bool autotune = false;
+    int force_tile = 0;                     // COL_TILE_* for every column pass (0: default / tuned)
+    std::map<std::string, int> tuned_tile;
+    std::map<int64_t, bool> tuned_solves;   // (type, nbatch) already tuned
+    // solves captured in CUDA graphs, keyed by (field, rhs, nbatch, type)
+    struct GraphKey {
+        const void* field;
+        const void* rhs;
+        int nbatch, type;
+        bool operator<(const GraphKey& o) const {
+            if (field != o.field) return field < o.field;
+            if (rhs != o.rhs) return rhs < o.rhs;
+            if (nbatch != o.nbatch) return nbatch < o.nbatch;
+            return type < o.type;
+        }
+    };
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+    cudaStream_t capture_stream = nullptr;
+    bool capturing = false;
+    void drop_graphs();
+    std::string pass_key(const flb::PassArgs& A, bool f64) const;
+    void autotune_passes(int type, int nbatch);
+    int solve_graph(double* field, double* rhs, int type, int nbatch);
     std::vector<cudaEvent_t> ev;          // 2 per pass of the last solve
     std::vector<double> pass_ms, pass_bytes;
     std::vector<long> pass_calls;

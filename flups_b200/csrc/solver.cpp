@@ -152,6 +152,8 @@ void Solver::dry_run(DirPlan p[3]) {
 }
 
 Solver::~Solver() {
+    drop_graphs();
+    if (capture_stream) cudaStreamDestroy(capture_stream);
     if (h2d_stream) {
         // copies of an async solve may still be in flight
         cudaStreamSynchronize(h2d_stream);
@@ -507,6 +509,12 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     fast_args(A, kind, in_f64, out_f64, c, r, mode);
     if (kind == 1) {
         c.tws = stage_table(L, f64);
+        if (force_tile) {
+            c.tile = force_tile;
+        } else if (!tuned_tile.empty()) {
+            auto it = tuned_tile.find(pass_key(A, f64));
+            if (it != tuned_tile.end()) c.tile = it->second;
+        }
         check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
         return;
     }
@@ -905,6 +913,7 @@ void Solver::ensure_buffers(int nbatch) {
             need = std::max(need, state_reals(k, nbatch));
         }
         if (need > buf_elems[b]) {
+            drop_graphs();  // captured solves point at the old arrays
             if (buf[b]) cudaFree(buf[b]);
             buf[b] = nullptr;
             check_cuda(cudaMalloc(&buf[b], need * es), "work buffer");
@@ -912,6 +921,11 @@ void Solver::ensure_buffers(int nbatch) {
         }
     }
     buf_batch = std::max(buf_batch, nbatch);
+}
+
+void Solver::drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
 }
 
 size_t Solver::device_bytes(int nbatch) const {
@@ -1032,8 +1046,10 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     FLB_CHECK(rhs != nullptr, "rhs is NULL");
     FLB_CHECK(nbatch >= 1, "nbatch must be >= 1");
     ensure_buffers(nbatch);
+    if (autotune) autotune_passes(type, nbatch);
     const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
-    const bool dev_in = is_device_ptr(rhs), dev_out = is_device_ptr(field);
+    // (a solve being captured has device arrays, checked before the capture)
+    const bool dev_in = capturing || is_device_ptr(rhs), dev_out = capturing || is_device_ptr(field);
     if ((!dev_in || !dev_out) && streamed_ok()) {
         solve_streamed(field, rhs, !dev_in, !dev_out, type, nbatch);
         return;
@@ -1155,6 +1171,120 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
     if (out_host) check_cuda(cudaStreamWaitEvent(stream, ev_out[ns - 1], 0), "stream wait");
     if (!async) check_cuda(cudaStreamSynchronize(stream), "solve");
     else check_cuda(cudaGetLastError(), "solve");
+}
+
+// ---------------------------------------------------------------- autotuning
+std::string Solver::pass_key(const PassArgs& A, bool f64) const {
+    char b[160];
+    snprintf(b, sizeof(b), "%d/%d/%d/%d/%d/%d/%d/%d/%d", f64 ? 1 : 0, A.axis, A.fused, A.st[0].M, A.n_src,
+             A.st[A.fused ? 1 : 0].n_store, A.n_a, A.n_b, A.ncomp);
+    return b;
+}
+
+// Time both CTA tiles of every column pass of a (type, nbatch) solve and keep
+// the faster.  The passes run on the solver's work arrays, whose contents are
+// dead between solves (the real passes overwrite them), so tuning needs no
+// extra memory; it synchronises the stream and runs once per signature.
+void Solver::autotune_passes(int type, int nbatch) {
+    const int64_t sk = (int64_t)nbatch * 4 + type;
+    if (tuned_solves.count(sk)) return;
+    tuned_solves[sk] = true;
+    const bool f64 = (precision == 64);
+    dry = true;
+    dry_passes.clear();
+    dry_flags.clear();
+    dry_names.clear();
+    dry_fast.clear();
+    do_fft_forward(nullptr, nbatch);
+    do_fft_backward_fused(nullptr, type, nbatch);
+    dry = false;
+    std::vector<PassArgs> passes = dry_passes;
+    std::vector<int> kinds = dry_fast;
+    dry_passes.clear();
+    dry_flags.clear();
+    dry_names.clear();
+    dry_fast.clear();
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "event");
+    check_cuda(cudaEventCreate(&e1), "event");
+    for (size_t i = 0; i < passes.size(); ++i) {
+        if (kinds[i] != 1) continue;
+        const PassArgs& A = passes[i];
+        const std::string key = pass_key(A, f64);
+        if (tuned_tile.count(key)) continue;
+        ColArgs c;
+        RowArgs r;
+        int mode = 0;
+        fast_args(A, 1, f64, f64, c, r, mode);
+        const int L = A.st[0].M;
+        c.tws = stage_table(L, f64);
+        float best = 1e30f;
+        int best_tile = COL_TILE_DEFAULT;
+        for (int tile : {COL_TILE_256, COL_TILE_128}) {
+            c.tile = tile;
+            check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "autotune launch");
+            check_cuda(cudaEventRecord(e0, stream), "event");
+            for (int k = 0; k < 3; ++k) check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "autotune launch");
+            check_cuda(cudaEventRecord(e1, stream), "event");
+            check_cuda(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.f;
+            check_cuda(cudaEventElapsedTime(&ms, e0, e1), "event");
+            if (ms < best) {
+                best = ms;
+                best_tile = tile;
+            }
+        }
+        tuned_tile[key] = best_tile;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+}
+
+// ---------------------------------------------------------------- CUDA graphs
+// A solve of device arrays is a fixed sequence of launches on the solver's
+// stream, so it can be captured once and replayed: the first call for a given
+// (field, rhs, nbatch, type) runs a plain solve (which allocates and tunes what
+// it needs), then captures a second one; later calls only launch the graph.
+int Solver::solve_graph(double* field, double* rhs, int type, int nbatch) {
+    if (!is_setup || !field || !rhs || nbatch < 1) return -1;
+    if (!is_device_ptr(field) || !is_device_ptr(rhs)) return -2;
+    GraphKey k{field, rhs, nbatch, type};
+    auto it = graphs.find(k);
+    if (it == graphs.end()) {
+        const bool keep_async = async;
+        async = true;
+        solve(field, rhs, type, nbatch);  // allocations, tuning, kernel attributes
+        // capture on a private stream (the legacy default stream cannot be captured)
+        if (!capture_stream) check_cuda(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking), "capture stream");
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        cudaStream_t user_stream = stream;
+        stream = capture_stream;
+        capturing = true;
+        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            solve(field, rhs, type, nbatch);
+            e = cudaStreamEndCapture(stream, &g);
+        }
+        capturing = false;
+        stream = user_stream;
+        async = keep_async;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            last_error = (int)e;
+            cudaGetLastError();
+            return -4;
+        }
+        it = graphs.emplace(k, ge).first;
+    }
+    const cudaError_t e = cudaGraphLaunch(it->second, stream);
+    if (e != cudaSuccess) {
+        last_error = (int)e;
+        return -4;
+    }
+    if (!async) check_cuda(cudaStreamSynchronize(stream), "graph solve");
+    return 0;
 }
 
 // ---------------------------------------------------------------- host-only description

@@ -112,6 +112,9 @@ def load_library(path=None):
         "flups_get_precision": (c_int, [vp]),
         "flups_set_async": (None, [vp, c_int]),
         "flups_synchronize": (None, [vp]),
+        "flups_b200_set_autotune": (None, [vp, c_int]),
+        "flups_b200_set_col_tile": (None, [vp, c_int]),
+        "flups_solve_graph": (c_int, [vp, vp, vp, c_int, c_int]),
         "flups_get_last_error": (c_int, [vp]),
         "flups_get_device_bytes": (c_size_t, [vp, c_int]),
         "flups_b200_plan_json": (c_int, [vp, c_int, c_int, ctypes.c_char_p, c_int]),
@@ -258,6 +261,20 @@ class Solver:
 
     def synchronize(self):
         _lib.flups_synchronize(self._solver)
+
+    def set_autotune(self, on):
+        _lib.flups_b200_set_autotune(self._solver, int(bool(on)))
+
+    def set_col_tile(self, tile):
+        """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""
+        _lib.flups_b200_set_col_tile(self._solver, int(tile))
+
+    def solve_graph(self, field, rhs, nbatch=1, solver_type=SolverType.STD):
+        """Device arrays only; replays a captured CUDA graph after the first call."""
+        rc = _lib.flups_solve_graph(self._solver, _ptr(field), _ptr(rhs), int(nbatch), int(solver_type))
+        if rc != 0:
+            raise RuntimeError(f"flups_solve_graph returned {rc} (CUDA error {self.last_error()})")
+        return field
 
     def setup(self, change_comm=False):
         _lib.flups_setup(self._solver, bool(change_comm))

@@ -75,6 +75,27 @@ int flups_b200_plan_json(struct Solver* s, int type, int nbatch, char* out, int 
  * For cross-checking the two kernel families. */
 void flups_b200_set_fast_kernels(struct Solver* s, int on);
 
+/* CTA-tile autotuning of the column passes (1 = on, default 0).  When on,
+ * the first solve of each (solver type, nbatch) times the two compiled tiles
+ * of every column pass on the solver's work arrays and keeps the faster one;
+ * that first call synchronises the stream.  No reference counterpart. */
+void flups_b200_set_autotune(struct Solver* s, int on);
+
+/* Force the CTA tile of every column pass: 0 = default or tuned, 1 = 256
+ * threads, 2 = 128 threads.  For cross-checking the tiles. */
+void flups_b200_set_col_tile(struct Solver* s, int tile);
+
+/* A solve (nbatch consecutive right-hand sides, as flups_solve_batch) of
+ * device arrays replayed from a CUDA graph.  The first call for a given
+ * (field, rhs, nbatch, type) runs one plain solve, then captures the next
+ * into a graph; later calls only launch the graph on the solver's stream.
+ * Graphs are dropped when the solver reallocates its work arrays and at
+ * cleanup.  Synchronises unless flups_set_async(s, 1).  Returns 0, -1 (not
+ * set up or bad arguments), -2 (host pointers) or -4 (CUDA error, also in
+ * flups_get_last_error).  No reference counterpart (the reference launches
+ * FFTW plans, src/Solver.cpp:1207-1272). */
+int flups_solve_graph(struct Solver* s, double* field, double* rhs, int nbatch, int type);
+
 /* One solve that allocates no device memory, for callers that cannot call
  * cudaMalloc while they run: code captured into a CUDA graph in the global
  * capture mode, real-time loops that must stay out of the allocator, and
