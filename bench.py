@@ -50,8 +50,10 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch"],
-                    help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum")
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve"],
+                    help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
+                         "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
     return ap.parse_args()
 
 
@@ -322,6 +324,64 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """Serving trace: Poisson arrivals at 500 req/s; grid n^3 cell-centred with n in
+    {32,...,256}; BC sets all-UNB, (PER,PER,UNB), (EVEN,UNB,UNB); HEJ_2 or LGF_2;
+    FP32 (0.8) or FP64 (0.2); right-hand sides are seeded Gaussian sums resident on
+    the device.  Runs the continuous-batching server from a cold cache, again with
+    every key's solver resident, and a serial server (one solve at a time, no
+    batching) on the same warm cache.  One step = the whole trace."""
+    import torch
+    from flups_b200.serving import GpuBackend, Request, Server, latency_stats, make_trace, rhs_pool, run_trace
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    sizes = (32, 48, 64, 96, 128, 192, 256)
+    pool = rhs_pool(sizes, per_size=4, device=dev)
+    torch.cuda.synchronize()
+    trace = make_trace(n_req=args.requests, rate=500.0, seed=5, sizes=sizes)
+    free, total = torch.cuda.mem_get_info()
+    budget = int(0.5 * free)
+    be = GpuBackend()
+
+    def finish_drop(h, reqs):
+        for r in reqs:
+            r.out = None  # results are complete; the caller would read them here
+    be.finish = finish_drop
+
+    def make(i, key, idx, ta):
+        rhs = pool[(key[0], idx)]
+        return Request(i, key, rhs, torch.empty_like(rhs), ta)
+
+    def run(srv):
+        srv.completed = []
+        wall = run_trace(srv, trace, make)
+        torch.cuda.synchronize()
+        st = latency_stats(srv.completed)
+        pts = sum(r.key[0] ** 3 for r in srv.completed)
+        return {"wall_s": wall, "solves_per_s": len(srv.completed) / wall, "pts_per_s": pts / wall,
+                "mean_batch": float(np.mean([r.batch for r in srv.completed])), **st}
+
+    srv = Server(be, budget, max_batch=16)
+    cold = run(srv)
+    cold.update({"setups": srv.setups, "evictions": srv.evictions})
+    warm = run(srv)
+    serial = Server(be, budget, max_batch=1, max_inflight=1)
+    serial.cache, serial.reserved = srv.cache, srv.reserved
+    ser = run(serial)
+    srv.close()
+    line = {
+        "metric": METRIC, "value": warm["pts_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": warm["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64 mix (0.8/0.2)", "data": "synthetic (seeded Gaussian sums, Poisson arrivals, seed 5)",
+        "config": {"workload": f"serving trace: {args.requests} requests at 500 req/s, n in {list(sizes)}, BC sets "
+                               "all-UNB/(PER,PER,UNB)/(EVEN,UNB,UNB), HEJ_2/LGF_2, fp32/fp64 0.8/0.2",
+                   "budget_bytes": budget, "max_batch": 16},
+        "p50_ms": warm["p50_ms"], "p99_ms": warm["p99_ms"],
+        "serve": {"continuous_warm": warm, "continuous_cold": cold, "serial_warm": ser},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -329,6 +389,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
         return
     import torch
     import torch.distributed as dist
