@@ -355,7 +355,11 @@ void Solver::fit_lines(PassArgs& A, int elem_bytes) const {
     A.lines_per_cta = 1;
     const size_t one = line_pass_smem(A, elem_bytes);
     FLB_CHECK(one <= 227 * 1024, "a line of this size does not fit in shared memory (%zu bytes)", one);
-    int tl = (int)std::min<size_t>(32, (200 * 1024) / one);
+    // tiles of about 50 KB (FP32, 4 CTAs per SM) or 100 KB (FP64, whose
+    // register count allows 2): several resident CTAs hide the barriers of
+    // the shared-memory stages
+    const size_t target = (elem_bytes == 4 ? 50 : 100) * 1024;
+    int tl = (int)std::min<size_t>(32, target / one);
     tl = std::max(tl, 1);
     const int64_t work = A.comps_together ? A.nlines : (int64_t)A.nlines * A.ncomp;
     if (tl > work) tl = (int)std::max<int64_t>(1, work);
