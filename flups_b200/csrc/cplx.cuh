@@ -289,16 +289,128 @@ template <typename C> __device__ __forceinline__ void dft32z(C* v) {
     for (int i = 0; i < 32; ++i) v[i] = t[i];
 }
 
-template <typename C> __device__ __forceinline__ void dft3(C* v) {
+template <bool INV = false, typename C> __device__ __forceinline__ void dft3(C* v) {
     using S = decltype(v[0].x);
     const S h = (S)0.5, s3 = (S)0.86602540378443864676;
     C a = cadd(v[1], v[2]);
-    C d = cmul_mi(csub(v[1], v[2]));
+    C d = INV ? cmul_pi(csub(v[1], v[2])) : cmul_mi(csub(v[1], v[2]));
     C t = csub(v[0], cscale(a, h));
     v[0] = cadd(v[0], a);
     C u = cscale(d, s3);
     v[1] = cadd(t, u);
     v[2] = csub(t, u);
+}
+template <bool INV = false, typename C> __device__ __forceinline__ void dft3(C& a0, C& a1, C& a2) {
+    C v[3] = {a0, a1, a2};
+    dft3<INV>(v);
+    a0 = v[0];
+    a1 = v[1];
+    a2 = v[2];
+}
+
+// W24^m = (cos(pi m/12), -sin(pi m/12)) for the m = n1*k2 products of dft24
+template <typename S> __device__ __forceinline__ void w24(int m, S& c, S& s) {
+    switch (m) {
+        case 1: c = (S)0.9659258262890682867497; s = -(S)0.2588190451025207623489; break;
+        case 2: c = (S)0.8660254037844386467637; s = -(S)0.5; break;
+        case 3: c = (S)0.7071067811865475244008; s = -(S)0.7071067811865475244008; break;
+        case 4: c = (S)0.5; s = -(S)0.8660254037844386467637; break;
+        case 5: c = (S)0.2588190451025207623489; s = -(S)0.9659258262890682867497; break;
+        case 7: c = -(S)0.2588190451025207623489; s = -(S)0.9659258262890682867497; break;
+        case 8: c = -(S)0.5; s = -(S)0.8660254037844386467637; break;
+        case 9: c = -(S)0.7071067811865475244008; s = -(S)0.7071067811865475244008; break;
+        case 10: c = -(S)0.8660254037844386467637; s = -(S)0.5; break;
+        case 11: c = -(S)0.9659258262890682867497; s = -(S)0.2588190451025207623489; break;
+        case 12: c = (S)-1; s = (S)0; break;
+        case 13: c = -(S)0.9659258262890682867497; s = (S)0.2588190451025207623489; break;
+        case 14: c = -(S)0.8660254037844386467637; s = (S)0.5; break;
+        default: c = (S)1; s = (S)0; break;
+    }
+}
+
+// DFT24 as 3 x 8: inner DFT8 over n2 of a[n1 + 3 n2], twiddle W24^{n1 k2},
+// outer DFT3 over n1; output k2 + 8 k1.  Z: inputs 12..23 are zero (then the
+// inner DFT8s see a zero upper half).
+template <bool INV = false, bool Z = false, typename C> __device__ __forceinline__ void dft24(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) {
+        C a[8];
+#pragma unroll
+        for (int n2 = 0; n2 < 8; ++n2) a[n2] = v[n1 + 3 * n2];
+        if constexpr (Z) dft8z(a);
+        else dft8<INV>(a);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) v[n1 + 3 * k2] = a[k2];
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < 3; ++n1) {
+#pragma unroll
+        for (int k2 = 1; k2 < 8; ++k2) {
+            if (n1 * k2 == 6) {
+                v[n1 + 3 * k2] = INV ? cmul_pi(v[n1 + 3 * k2]) : cmul_mi(v[n1 + 3 * k2]);
+            } else {
+                S c, s;
+                w24<S>(n1 * k2, c, s);
+                v[n1 + 3 * k2] = cmul(v[n1 + 3 * k2], mkc(c, INV ? -s : s));
+            }
+        }
+    }
+    C t[24];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        C a0 = v[3 * k2], a1 = v[1 + 3 * k2], a2 = v[2 + 3 * k2];
+        dft3<INV>(a0, a1, a2);
+        t[k2] = a0; t[k2 + 8] = a1; t[k2 + 16] = a2;
+    }
+#pragma unroll
+    for (int i = 0; i < 24; ++i) v[i] = t[i];
+}
+
+// W12^m = (cos(pi m/6), -sin(pi m/6))
+template <typename S> __device__ __forceinline__ void w12(int m, S& c, S& s) {
+    switch (m) {
+        case 1: c = (S)0.8660254037844386467637; s = -(S)0.5; break;
+        case 2: c = (S)0.5; s = -(S)0.8660254037844386467637; break;
+        case 4: c = -(S)0.5; s = -(S)0.8660254037844386467637; break;
+        case 5: c = -(S)0.8660254037844386467637; s = -(S)0.5; break;
+        case 6: c = (S)-1; s = (S)0; break;
+        default: c = (S)1; s = (S)0; break;
+    }
+}
+
+// DFT12 as 3 x 4 (same layout as dft24); Z: inputs 6..11 are zero
+template <bool INV = false, bool Z = false, typename C> __device__ __forceinline__ void dft12(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) {
+        C a0 = v[n1], a1 = v[n1 + 3], a2 = v[n1 + 6], a3 = v[n1 + 9];
+        if constexpr (Z) dft4z(a0, a1, a2, a3);
+        else dft4<INV>(a0, a1, a2, a3);
+        v[n1] = a0; v[n1 + 3] = a1; v[n1 + 6] = a2; v[n1 + 9] = a3;
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < 3; ++n1) {
+#pragma unroll
+        for (int k2 = 1; k2 < 4; ++k2) {
+            if (n1 * k2 == 3) {
+                v[n1 + 3 * k2] = INV ? cmul_pi(v[n1 + 3 * k2]) : cmul_mi(v[n1 + 3 * k2]);
+            } else {
+                S c, s;
+                w12<S>(n1 * k2, c, s);
+                v[n1 + 3 * k2] = cmul(v[n1 + 3 * k2], mkc(c, INV ? -s : s));
+            }
+        }
+    }
+    C t[12];
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        C a0 = v[3 * k2], a1 = v[1 + 3 * k2], a2 = v[2 + 3 * k2];
+        dft3<INV>(a0, a1, a2);
+        t[k2] = a0; t[k2 + 4] = a1; t[k2 + 8] = a2;
+    }
+#pragma unroll
+    for (int i = 0; i < 12; ++i) v[i] = t[i];
 }
 
 template <typename C> __device__ __forceinline__ void dft5(C* v) {

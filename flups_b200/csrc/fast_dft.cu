@@ -5,12 +5,25 @@
 
 namespace flb {
 
-bool fast_col_supported(int L) { return L == 64 || L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048; }
-bool fast_row_supported(int L) { return L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048 || L == 4096; }
+// powers of two and 3 x powers of two
+bool fast_col_supported(int L) {
+    switch (L) {
+        case 64: case 128: case 256: case 512: case 1024: case 2048:
+        case 96: case 192: case 384: case 768: case 1536: return true;
+    }
+    return false;
+}
+bool fast_row_supported(int L) {
+    switch (L) {
+        case 128: case 256: case 512: case 1024: case 2048: case 4096:
+        case 96: case 192: case 384: case 768: case 1536: case 3072: return true;
+    }
+    return false;
+}
 
-int fast_radix1(int f64) { return f64 ? 16 : 32; }
+int fast_radix1(int f64, int n) { return fast_radix1_of(n, f64); }
 
-int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1(f64)); }
+int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1_of(n, f64)); }
 
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };

@@ -42,21 +42,28 @@ struct RowArgs {
 bool fast_col_supported(int L);
 bool fast_row_supported(int L);
 
-// First radix of the register DFTs: 32 in FP32, 16 in FP64.
-int fast_radix1(int f64);
+// First radix of the register DFTs for an n-point line: 32 in FP32 and 16 in
+// FP64 for powers of two; 24 (3 x 8) in FP32 and 12 (3 x 4) in FP64 for 3 x 2^k.
+__host__ __device__ constexpr int fast_radix1_of(int n, int f64) {
+    return (n % 3 == 0) ? (f64 ? 12 : 24) : (f64 ? 16 : 32);
+}
+int fast_radix1(int f64, int n);
+// radix of a later Stockham stage: the largest common divisor of what is left
+// of the line (n / Ns) and the first radix
+__host__ __device__ constexpr int fast_gcd(int a, int b) { return b == 0 ? a : fast_gcd(b, a % b); }
 // Complex entries of the later-stage twiddle table of an n-point register DFT.
 int fast_stage_table_len(int n, int f64);
 // Entry e of that table is W_M^q = exp(-2 pi i q / M); sets q and M.
 // Layout: one block of n entries per stage after the first (Ns = r1, r1*Rs, ...
-// with Rs = min(n/Ns, r1)); in a block, pair (b * Rs/2 + rp) * P + p (P = n/r1)
+// with Rs = gcd(n/Ns, r1)); in a block, pair (b * Rs/2 + rp) * P + p (P = n/r1)
 // holds W_{Ns Rs}^{r k} for r = 2rp, 2rp+1 and k = (p + P b) mod Ns: the
 // twiddles of butterfly b of thread p, two per 16-byte (FP32) load.
 __host__ __device__ inline void fast_stage_exponent(int n, int r1, int e, int* q, int* M) {
     const int P = n / r1;
     const int s = e / n, w = e % n;
     int Ns = r1;
-    for (int i = 0; i < s; ++i) Ns *= (n / Ns < r1) ? n / Ns : r1;
-    const int Rs = (n / Ns < r1) ? n / Ns : r1;
+    for (int i = 0; i < s; ++i) Ns *= fast_gcd(n / Ns, r1);
+    const int Rs = fast_gcd(n / Ns, r1);
     const int pair = w / 2, half = w % 2;
     const int p = pair % P, t = pair / P;
     const int rp = t % (Rs / 2), b = t / (Rs / 2);

@@ -37,6 +37,8 @@ __device__ __forceinline__ void dftr(C* v) {
     else if constexpr (R == 8) dft8<INV>(v);
     else if constexpr (R == 16) dft16<INV>(v);
     else if constexpr (R == 32) dft32<INV>(v);
+    else if constexpr (R == 24) dft24<INV>(v);
+    else if constexpr (R == 12) dft12<INV>(v);
 }
 
 // radix-R DFT of v whose upper half is zero
@@ -47,6 +49,8 @@ __device__ __forceinline__ void dftz(C* v) {
     else if constexpr (R == 8) dft8z(v);
     else if constexpr (R == 16) dft16z(v);
     else if constexpr (R == 32) dft32z(v);
+    else if constexpr (R == 24) dft24<false, true>(v);
+    else if constexpr (R == 12) dft12<false, true>(v);
 }
 
 // two consecutive complex twiddles of a stage table, from shared memory
@@ -69,7 +73,7 @@ template <bool SM> struct TwPair<double, SM> {
 // complex entries of the later-stage table of an n-point DFT with first radix r1
 __host__ __device__ constexpr int stage_table_entries(int n, int r1) {
     int stages = 0;
-    for (int Ns = r1; Ns < n; Ns *= (n / Ns < r1) ? n / Ns : r1) ++stages;
+    for (int Ns = r1; Ns < n; Ns *= fast_gcd(n / Ns, r1)) ++stages;
     return stages * n;
 }
 
@@ -94,7 +98,8 @@ struct RegFFT {
     // Stockham stage with Ns-point sub-transforms done; tws = this stage's table
     template <int Ns, bool INV>
     __device__ static __forceinline__ void stages(C* v, C* sm, int p, const C* __restrict__ tws) {
-        constexpr int Rs = (L / Ns < R1) ? (L / Ns) : R1;
+        constexpr int Rs = fast_gcd(L / Ns, R1);
+        static_assert(Rs >= 2 && Rs % 2 == 0, "a later stage needs an even radix");
         constexpr int NB = R1 / Rs;  // butterflies per thread
         constexpr int MR = L / Rs;
         C t[R1];
@@ -159,10 +164,15 @@ struct RegFFT {
         else dftr<R1, INV>(v);
         if constexpr (P > 1) {
             __syncthreads();
-            // sw(p R1 + k) = sw(p R1) + k for k < R1 <= 32
-            C* d0 = sm + sw(p * R1);
+            // sw(p R1 + k) = sw(p R1) + k for k < R1 when R1 divides 32
+            if constexpr (32 % R1 == 0) {
+                C* d0 = sm + sw(p * R1);
 #pragma unroll
-            for (int k = 0; k < R1; ++k) d0[k] = v[k];
+                for (int k = 0; k < R1; ++k) d0[k] = v[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < R1; ++k) sm[sw(p * R1 + k)] = v[k];
+            }
             __syncthreads();
             stages<R1, INV>(v, sm, p, tws);
         }
@@ -419,7 +429,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
             const int k = p + F::P * r;
             if (k >= a.nout) continue;
             const C zk = v[r];
-            const C zm = cconj(line[F::sw((LH - k) & (LH - 1))]);
+            const C zm = cconj(line[F::sw(k == 0 ? 0 : LH - k)]);
             const C e = cadd(zk, zm);
             const C d = csub(zk, zm);
             const C w = cmul(tw[F::P * r], d);  // W_L^k (Z_k - conj Z_{LH-k})
@@ -475,7 +485,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     for (int r = 0; r < R1; ++r) {
         const int k = p + F::P * r;
         C xk = line[F::sw(k)];
-        C xm = line[F::sw((LH - k) & (LH - 1))];
+        C xm = line[F::sw(k == 0 ? 0 : LH - k)];
         if (k == 0) {
             xm = xlh;
             xk.y = (T)0;
@@ -534,7 +544,7 @@ inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
 // the autotuner (Solver::autotune_passes) may pick the other per pass.
 template <typename T, int L, int THREADS, int MODE, int SH>
 inline cudaError_t launch_col_threads(const ColArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
+    constexpr int R1 = fast_radix1_of(L, sizeof(T) == 8);
     constexpr int TX = THREADS / (L / R1);
     static_assert(TX >= 1, "tile narrower than one column");
     return launch_col_t<T, L, R1, TX, MODE, SH>(a, ncomp, s);
@@ -556,6 +566,11 @@ inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStrea
         case 512: return wide ? launch_col_threads<T, 512, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 512, 128, MODE, SH>(a, ncomp, s);
         case 1024: return wide ? launch_col_threads<T, 1024, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 1024, 128, MODE, SH>(a, ncomp, s);
         case 2048: return wide ? launch_col_threads<T, 2048, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 2048, 128, MODE, SH>(a, ncomp, s);
+        case 96: return wide ? launch_col_threads<T, 96, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 96, 128, MODE, SH>(a, ncomp, s);
+        case 192: return wide ? launch_col_threads<T, 192, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 192, 128, MODE, SH>(a, ncomp, s);
+        case 384: return wide ? launch_col_threads<T, 384, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 384, 128, MODE, SH>(a, ncomp, s);
+        case 768: return wide ? launch_col_threads<T, 768, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 768, 128, MODE, SH>(a, ncomp, s);
+        case 1536: return wide ? launch_col_threads<T, 1536, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 1536, 128, MODE, SH>(a, ncomp, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -590,14 +605,20 @@ inline cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
 
 template <typename T, typename XT, bool C2R, bool HALF>
 inline cudaError_t launch_row_len(int L, const RowArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = sizeof(T) == 4 ? 32 : 16;
+    constexpr bool F64 = sizeof(T) == 8;
     switch (L) {
-        case 128: return launch_row_t<T, XT, 64, R1, C2R, HALF>(a, ncomp, s);
-        case 256: return launch_row_t<T, XT, 128, R1, C2R, HALF>(a, ncomp, s);
-        case 512: return launch_row_t<T, XT, 256, R1, C2R, HALF>(a, ncomp, s);
-        case 1024: return launch_row_t<T, XT, 512, R1, C2R, HALF>(a, ncomp, s);
-        case 2048: return launch_row_t<T, XT, 1024, R1, C2R, HALF>(a, ncomp, s);
-        case 4096: return launch_row_t<T, XT, 2048, R1, C2R, HALF>(a, ncomp, s);
+        case 128: return launch_row_t<T, XT, 64, fast_radix1_of(64, F64), C2R, HALF>(a, ncomp, s);
+        case 256: return launch_row_t<T, XT, 128, fast_radix1_of(128, F64), C2R, HALF>(a, ncomp, s);
+        case 512: return launch_row_t<T, XT, 256, fast_radix1_of(256, F64), C2R, HALF>(a, ncomp, s);
+        case 1024: return launch_row_t<T, XT, 512, fast_radix1_of(512, F64), C2R, HALF>(a, ncomp, s);
+        case 2048: return launch_row_t<T, XT, 1024, fast_radix1_of(1024, F64), C2R, HALF>(a, ncomp, s);
+        case 4096: return launch_row_t<T, XT, 2048, fast_radix1_of(2048, F64), C2R, HALF>(a, ncomp, s);
+        case 96: return launch_row_t<T, XT, 48, fast_radix1_of(48, F64), C2R, HALF>(a, ncomp, s);
+        case 192: return launch_row_t<T, XT, 96, fast_radix1_of(96, F64), C2R, HALF>(a, ncomp, s);
+        case 384: return launch_row_t<T, XT, 192, fast_radix1_of(192, F64), C2R, HALF>(a, ncomp, s);
+        case 768: return launch_row_t<T, XT, 384, fast_radix1_of(384, F64), C2R, HALF>(a, ncomp, s);
+        case 1536: return launch_row_t<T, XT, 768, fast_radix1_of(768, F64), C2R, HALF>(a, ncomp, s);
+        case 3072: return launch_row_t<T, XT, 1536, fast_radix1_of(1536, F64), C2R, HALF>(a, ncomp, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -170,7 +170,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     cudaStream_t st = s->stream;
     for (const TwSlot& t : slots) {
         const int nb = std::min(1184, (t.len + 255) / 256);
-        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, fast_radix1(f64 ? 1 : 0), f64 ? 1 : 0);
+        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, fast_radix1(f64 ? 1 : 0, t.n), f64 ? 1 : 0);
     }
     auto tw_of = [&](int n, int stage) { return (const void*)(base + slot_for(n, stage)); };
     for (size_t i = 0; i < passes.size(); ++i) {

@@ -531,7 +531,7 @@ const void* Solver::stage_table(int n, bool f64) {
     const int64_t key = ((int64_t)1 << 40) + (int64_t)n * 2 + (f64 ? 1 : 0);
     auto it = twiddles.find(key);
     if (it != twiddles.end()) return it->second;
-    const int len = fast_stage_table_len(n, f64 ? 1 : 0), r1 = fast_radix1(f64 ? 1 : 0);
+    const int len = fast_stage_table_len(n, f64 ? 1 : 0), r1 = fast_radix1(f64 ? 1 : 0, n);
     std::vector<double> w(2 * (size_t)std::max(len, 1), 0.0);
     for (int e = 0; e < len; ++e) {
         int q = 0, M = 1;

@@ -51,6 +51,10 @@ CASES = [
     ("ppu64_hej4", [64] * 3, 1, PPU, CELL_CENTER, HEJ_4),
     ("node65_unb", [65] * 3, 1, UNB3, NODE_CENTER, CHAT_2),
     ("vector3_unb64", [64] * 3, 3, [[[4] * 3, [4] * 3]] * 3, CELL_CENTER, LGF_2),
+    # 3 x 2^k lines (radix-3 first stage): 96, 192, 384 points
+    ("unb48_hej2_r3", [48] * 3, 1, UNB3, CELL_CENTER, HEJ_2),
+    ("unb96_48_192_r3", [96, 48, 192], 1, UNB3, CELL_CENTER, LGF_2),
+    ("ppu96_hej4_r3", [96, 96, 48], 1, PPU, CELL_CENTER, HEJ_4),
 ]
 
 
