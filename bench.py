@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "config2", "config3"],
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
@@ -324,6 +324,144 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+def config2_rhs(dev):
+    """513 x 257 x 257 nodes at i h (h = 1/256) on [0,2]x[0,1]x[0,1]: sum of 8 Gaussians,
+    centres uniform in the domain shrunk by 0.2 L per side, sigma in [0.03,0.08], a in [-1,1]."""
+    import torch
+    rng = np.random.default_rng(2)
+    h = 1.0 / 256
+    n = (513, 257, 257)
+    L = (2.0, 1.0, 1.0)
+    ax = [torch.arange(n[d], dtype=torch.float64, device=dev) * h for d in range(3)]
+    f = torch.zeros((n[2], n[1], n[0]), dtype=torch.float64, device=dev)
+    for _ in range(8):
+        c = [rng.uniform(0.2 * L[d], 0.8 * L[d]) for d in range(3)]
+        sg = rng.uniform(0.03, 0.08)
+        a = rng.uniform(-1.0, 1.0)
+        g = [torch.exp(-(ax[d] - c[d]) ** 2 / sg ** 2) for d in range(3)]
+        f += a * g[2][:, None, None] * g[1][None, :, None] * g[0][None, None, :]
+    return f
+
+
+def config3_rhs(n, dev):
+    """Vortex ring on n^3 cells of [0,1]^3: centre (0.5,0.5,0.5), axis z, radius
+    R(theta) = 0.25 (1 + sum_{m=1..8} a_m cos(m theta + phi_m)), a_m in [-1e-3,1e-3],
+    phi_m in [0,2 pi); azimuthal vorticity Gamma/(pi s^2) exp(-d^2/s^2), Gamma = 1,
+    s = 0.03, d the distance to the core line.  Returns [3][z][y][x]."""
+    import torch
+    rng = np.random.default_rng(3)
+    am = rng.uniform(-1e-3, 1e-3, 8)
+    ph = rng.uniform(0.0, 2 * np.pi, 8)
+    x = (torch.arange(n, dtype=torch.float64, device=dev) + 0.5) / n - 0.5
+    Z, Y, X = torch.meshgrid(x, x, x, indexing="ij")
+    rho = torch.sqrt(X * X + Y * Y)
+    th = torch.atan2(Y, X)
+    R = torch.full_like(th, 0.25)
+    for m in range(8):
+        R = R + 0.25 * am[m] * torch.cos((m + 1) * th + ph[m])
+    d2 = (rho - R) ** 2 + Z * Z
+    s = 0.03
+    w = (1.0 / (np.pi * s * s)) * torch.exp(-d2 / (s * s))
+    out = torch.stack([-torch.sin(th) * w, torch.cos(th) * w, torch.zeros_like(w)])
+    return out.contiguous()
+
+
+def fast_flags(stats, plan):
+    """Kernel family per timed pass: from the host-side plan where it lists the
+    same passes; the split ROT passes (rot_fwd / rot_curl / rot_bwd) are named."""
+    planned = [q.get("fast", 0) for q in plan.get("passes", []) if q.get("name") != "green"]
+    if len(planned) == len(stats):
+        return planned
+    by_name = {q.get("name"): q.get("fast", 0) for q in plan.get("passes", [])}
+    return [1 if p["name"] in ("rot_fwd", "rot_bwd", "rot_curl") else by_name.get(p["name"], 0) for p in stats]
+
+
+def run_config(args):
+    """Config 2 (node-centred 513x257x257, EVEN/ODD x, PER y, UNB z, HEJ_4) or
+    config 3 (384^3 cell, all UNB, LGF_4, ROT with the spectral curl, 3 components):
+    FP32 and FP64 solves of device arrays, the FP32 error against the FP64 mode,
+    and the per-pass times (which show the general line-pass kernel where the
+    register DFTs do not apply)."""
+    import torch
+    from flups_b200 import pyflups as pf
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    B = pf.BoundaryType
+    if args.workload == "config2":
+        nglob, lda, typ = [513, 257, 257], 1, 0
+        bcs = [[B.EVEN, B.ODD], [B.PER, B.PER], [B.UNB, B.UNB]]
+        h, L, center, kernel, odiff = [1 / 256] * 3, [2.0, 1.0, 1.0], pf.CenterType.NODE_CENTER, "HEJ_4", pf.DiffType.NOD
+        rhs = config2_rhs(dev)
+        name = "config 2: 513x257x257 node-centred, EVEN/ODD x, PER y, UNB z, HEJ_4 (alpha 2)"
+    else:
+        n = 384
+        nglob, lda, typ = [n] * 3, 3, 1
+        bcs = [[[B.UNB] * 3, [B.UNB] * 3]] * 3
+        h, L, center, kernel, odiff = [1 / n] * 3, [1.0] * 3, pf.CenterType.CELL_CENTER, "LGF_4", pf.DiffType.SPE
+        rhs = config3_rhs(n, dev)
+        name = "config 3: 384^3 cell, all UNB, LGF_4, ROT (spectral curl), 3-component vortex ring"
+    torch.cuda.synchronize()
+    res = {}
+    outs = {}
+    for prec in (32, 64):
+        t = pf.Topology(0, lda, nglob)
+        s = pf.Solver(t, bcs, h, L, order_diff=odiff, center_type=[center] * 3)
+        s.set_green_type(pf.GreenType[kernel])
+        s.set_precision(prec)
+        s.set_stream(stream)
+        s.set_async(True)
+        t0 = time.perf_counter()
+        s.setup()
+        setup_s = time.perf_counter() - t0
+        out = torch.empty_like(rhs)
+        with torch.cuda.stream(stream):
+            for _ in range(max(3, args.warmup)):
+                s.solve(out, rhs, typ)
+        stream.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for a, b in evs:
+            a.record(stream)
+            s.solve(out, rhs, typ)
+            b.record(stream)
+        stream.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        s.set_pass_timing(True)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                s.solve(out, rhs, typ)
+        stream.synchronize()
+        stats = s.pass_stats()
+        plan = s.plan_json(typ, 1)
+        outs[prec] = out.clone()
+        res[prec] = {"ms_per_solve": float(np.mean(ms)), "p50_ms": float(np.percentile(ms, 50)),
+                     "p99_ms": float(np.percentile(ms, 99)), "setup_s": setup_s,
+                     "passes": [{"name": p["name"], "ms": p["ms_total"] / max(1, p["calls"]), "bytes": p["bytes"],
+                                 "kernel": ("register DFT" if f else "line pass")}
+                                for p, f in zip(stats, fast_flags(stats, plan))]}
+        del s, t
+        torch.cuda.empty_cache()
+    d = outs[32] - outs[64]
+    rel_l2 = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(outs[64]))
+    rel_linf = float(d.abs().max() / outs[64].abs().max())
+    pts = nglob[0] * nglob[1] * nglob[2]
+    peak, peak_kind = measured_peaks()
+    tot = sum(p["bytes"] for p in res[32]["passes"])
+    ms32 = res[32]["ms_per_solve"]
+    line = {
+        "metric": METRIC, "value": pts / (ms32 * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)", "config": {"workload": name, "grid": nglob, "lda": lda},
+        "p50_ms": res[32]["p50_ms"], "p99_ms": res[32]["p99_ms"],
+        "accuracy": {"fp32_rel_l2_vs_fp64": rel_l2, "fp32_rel_linf_vs_fp64": rel_linf},
+        "fp64": {"value": pts / (res[64]["ms_per_solve"] * 1e-3), "ms_per_step": res[64]["ms_per_solve"]},
+        "roofline": {"bound": "hbm", "kernel": "whole solve", "achieved": tot / (ms32 * 1e-3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": tot / (ms32 * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None},
+        "detail": res,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """Serving trace: Poisson arrivals at 500 req/s; grid n^3 cell-centred with n in
     {32,...,256}; BC sets all-UNB, (PER,PER,UNB), (EVEN,UNB,UNB); HEJ_2 or LGF_2;
@@ -392,6 +530,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload in ("config2", "config3"):
+        run_config(args)
         return
     import torch
     import torch.distributed as dist

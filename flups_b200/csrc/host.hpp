@@ -212,6 +212,11 @@ struct Solver {
     void fit_lines(flb::PassArgs& A, int elem_bytes) const;
     flb::MultSpec mult_spec(int type) const;
     void run_pass(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64, const char* name = "pass");
+    int timed_begin(const char* name, double bytes);
+    void timed_end(int k);
+    bool rot_split(int nbatch);
+    void* spec_buf = nullptr;             // full spectrum of a split ROT solve
+    size_t spec_bytes = 0;
     void collect_timing();
     void check_cuda(cudaError_t e, const char* what);
     void do_fft_forward(const double* user_in, int nbatch);

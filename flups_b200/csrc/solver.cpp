@@ -20,6 +20,7 @@
 
 #include "fast_dft.h"
 #include "host.hpp"
+#include "rot.h"
 
 using namespace flb;
 
@@ -165,6 +166,7 @@ Solver::~Solver() {
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
     if (stage_out) cudaFree(stage_out);
+    if (spec_buf) cudaFree(spec_buf);
     if (h2d_stream) {
         for (int k = 0; k < kSlabs; ++k) {
             cudaEventDestroy(ev_in[k]);
@@ -606,32 +608,40 @@ void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, 
     }
     for (int s2 = 0; s2 <= A.fused; ++s2)
         if (!A.st[s2].tw) A.st[s2].tw = twiddle(A.st[s2].M, f64);
-    const int k = pass_idx++;
-    if (timing) {
-        // algorithmic bytes: source and kept output lines once, the folded Green's spectrum once
-        const int64_t nc = A.comps_together ? (int64_t)A.ncomp : (int64_t)A.ncomp;
-        const double es = f64 ? 8.0 : 4.0;
-        const LineStage& last = A.st[A.fused ? 1 : 0];
-        double bytes = (double)A.n_src * A.nlines * nc * (A.st[0].in_cplx ? 2 : 1) * (in_f64 ? 8.0 : 4.0) +
-                       (double)last.n_store * A.nlines * nc * (last.out_cplx ? 2 : 1) * (out_f64 ? 8.0 : 4.0);
-        if (A.fused) bytes += (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
-        if ((int)pass_ms.size() <= k) {
-            pass_ms.resize(k + 1, 0.0);
-            pass_bytes.resize(k + 1, 0.0);
-            pass_calls.resize(k + 1, 0);
-            pass_names.resize(k + 1);
-        }
-        pass_bytes[k] = bytes;
-        pass_names[k] = name;
-        while ((int)ev.size() < 2 * (k + 1)) {
-            cudaEvent_t e;
-            check_cuda(cudaEventCreate(&e), "event");
-            ev.push_back(e);
-        }
-        cudaEventRecord(ev[2 * k], stream);
-    }
+    // algorithmic bytes: source and kept output lines once, the folded Green's spectrum once
+    const int64_t nc = A.ncomp;
+    const double es = f64 ? 8.0 : 4.0;
+    const LineStage& last = A.st[A.fused ? 1 : 0];
+    double bytes = (double)A.n_src * A.nlines * nc * (A.st[0].in_cplx ? 2 : 1) * (in_f64 ? 8.0 : 4.0) +
+                   (double)last.n_store * A.nlines * nc * (last.out_cplx ? 2 : 1) * (out_f64 ? 8.0 : 4.0);
+    if (A.fused) bytes += (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
+    const int k = timed_begin(name, bytes);
     if (fk) launch_fast(A, fk, f64, in_f64, out_f64);
     else check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
+    timed_end(k);
+}
+
+int Solver::timed_begin(const char* name, double bytes) {
+    const int k = pass_idx++;
+    if (!timing) return k;
+    if ((int)pass_ms.size() <= k) {
+        pass_ms.resize(k + 1, 0.0);
+        pass_bytes.resize(k + 1, 0.0);
+        pass_calls.resize(k + 1, 0);
+        pass_names.resize(k + 1);
+    }
+    pass_bytes[k] = bytes;
+    pass_names[k] = name;
+    while ((int)ev.size() < 2 * (k + 1)) {
+        cudaEvent_t e;
+        check_cuda(cudaEventCreate(&e), "event");
+        ev.push_back(e);
+    }
+    cudaEventRecord(ev[2 * k], stream);
+    return k;
+}
+
+void Solver::timed_end(int k) {
     if (timing) cudaEventRecord(ev[2 * k + 1], stream);
 }
 
@@ -983,10 +993,67 @@ void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
     do_backward(user_out, type, nbatch);
 }
 
+// ROT with the register DFTs on the last direction: forward DFT of the three
+// components into the full spectrum, the pointwise curl and Green's multiply
+// (rot.cu), inverse DFT back.  The general fused pass does the same on lines
+// in shared memory; splitting it lets both transforms run at the DFTs' speed
+// at the price of writing and reading the spectrum once.
+bool Solver::rot_split(int nbatch) {
+    if (dry || !use_fast) return false;
+    const bool f64 = (precision == 64);
+    const int es = f64 ? 8 : 4;
+    const int ipl = ndim - 1;
+    const DirPlan& p = fwd[ipl];
+    PassArgs F = base_pass(p.dim, st[ipl], lda * nbatch, lda);
+    F.st[0] = stage_forward(p, ipl, f64);
+    set_strides_internal(F.in_str, F.in_cstr, st[ipl]);
+    set_strides_internal(F.out_str, F.out_cstr, st[ndim]);
+    PassArgs Bk = base_pass(p.dim, st[ndim], lda * nbatch, lda);
+    Bk.st[0] = stage_backward(dif[ipl], p, ipl, f64);
+    set_strides_internal(Bk.in_str, Bk.in_cstr, st[ndim]);
+    set_strides_internal(Bk.out_str, Bk.out_cstr, st[ipl]);
+    // the decision is taken on the layout (pointers are checked again at launch)
+    const bool keep = dry;
+    dry = true;
+    const bool ok = fast_kind(F, f64, f64, f64) == 1 && fast_kind(Bk, f64, f64, f64) == 1;
+    dry = keep;
+    if (!ok) return false;
+    const size_t need = state_reals(ndim, nbatch) * es;
+    if (spec_bytes < need) {
+        drop_graphs();
+        if (spec_buf) cudaFree(spec_buf);
+        spec_buf = nullptr;
+        check_cuda(cudaMalloc(&spec_buf, need), "spectrum array");
+        spec_bytes = need;
+    }
+    F.in = buf[(ipl - 1) % 2];
+    F.out = spec_buf;
+    fit_lines(F, es);
+    run_pass(F, f64, f64, f64, "rot_fwd");
+    RotArgs R;
+    memset(&R, 0, sizeof(R));
+    R.data = spec_buf;
+    for (int d = 0; d < 3; ++d) R.n[d] = st[ndim].n[d];
+    set_strides_internal(R.str, R.cstr, st[ndim]);
+    R.nbatch = nbatch;
+    R.mult = mult_spec(ROT);
+    const double rbytes = 2.0 * (double)st[ndim].n[0] * st[ndim].n[1] * st[ndim].n[2] * 2 * es * 3 * nbatch +
+                          (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
+    const int k = timed_begin("rot_curl", rbytes);
+    check_cuda(launch_rot_mult(R, f64 ? 1 : 0, stream), "curl launch");
+    timed_end(k);
+    Bk.in = spec_buf;
+    Bk.out = buf[(ipl - 1) % 2];
+    fit_lines(Bk, es);
+    run_pass(Bk, f64, f64, f64, "rot_bwd");
+    return true;
+}
+
 void Solver::do_fused(int type, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const int ipl = ndim - 1;
+    if (type == ROT && rot_split(nbatch)) return;
     {
         // fused: forward ndim-1, multiply, backward ndim-1 (in place on state ndim-1)
         const DirPlan& p = fwd[ipl];

@@ -73,3 +73,21 @@ def test_fast_fp32_matches_oracle_and_general_engine(name, nglob, lda, bcv, cent
     assert rel_l2(got, ref) <= 2e-6
     assert rel_l2(gen, ref) <= 2e-6
     assert rel_l2(got, gen) <= 2e-6
+
+
+@pytest.mark.parametrize("n,odiff,kernel", [(32, 1, LGF_2), (48, 2, HEJ_2), (64, 4, CHAT_2)])
+def test_rot_split_matches_oracle(n, odiff, kernel):
+    """ROT solves whose last direction runs through the register DFTs are split
+    into forward DFT, pointwise curl and Green's multiply, inverse DFT: FP64
+    against the oracle (<= 1e-12), FP32 against the FP64 mode (<= 2e-6)."""
+    from gpu_helpers import gpu_solve
+    nglob = [n] * 3
+    bcv = [[[4] * 3, [4] * 3]] * 3
+    h = [1.0 / n] * 3
+    L = [1.0] * 3
+    rhs = _rhs(nglob, 3, seed=11)
+    got = gpu_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff)
+    ref = oracle_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff)
+    assert rel_l2(got, ref) <= 1e-12
+    got32 = gpu_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff, precision=32)
+    assert rel_l2(got32, got) <= 2e-6
