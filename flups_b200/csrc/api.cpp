@@ -185,30 +185,23 @@ void flups_set_alpha(Solver* s, const double alpha) {
     s->alpha = alpha;
 }
 double* flups_get_innerBuffer(Solver* s) {
-    FLB_CHECK(false, "flups_get_innerBuffer is not provided by this library yet");
-    return nullptr;
+    s->ensure_inner();
+    return s->inner;
 }
 Topology* flups_get_innerTopo_physical(Solver* s) {
-    FLB_CHECK(false, "flups_get_innerTopo_physical is not provided by this library yet");
-    return nullptr;
+    s->ensure_inner();
+    return s->topo_inner_phys;
 }
 Topology* flups_get_innerTopo_spectral(Solver* s) {
-    FLB_CHECK(false, "flups_get_innerTopo_spectral is not provided by this library yet");
-    return nullptr;
+    s->ensure_inner();
+    return s->topo_spec;
 }
+// the inner physical layout is the user layout: there is no first topology
+// switch to skip (kept as a no-op flag for callers of the reference API)
 void flups_skip_firstSwitchtopo(Solver* s) { s->skip_st0 = true; }
-void flups_do_copy(Solver* s, const Topology* topo, double* data, const int sign) {
-    (void)s; (void)topo; (void)data; (void)sign;
-    FLB_CHECK(false, "flups_do_copy is not provided by this library yet");
-}
-void flups_do_FFT(Solver* s, double* data, const int sign) {
-    (void)s; (void)data; (void)sign;
-    FLB_CHECK(false, "flups_do_FFT is not provided by this library yet");
-}
-void flups_do_mult(Solver* s, double* data, const FLUPS_SolverType type) {
-    (void)s; (void)data; (void)type;
-    FLB_CHECK(false, "flups_do_mult is not provided by this library yet");
-}
+void flups_do_copy(Solver* s, const Topology* topo, double* data, const int sign) { s->adv_copy(topo, data, sign); }
+void flups_do_FFT(Solver* s, double* data, const int sign) { s->adv_fft(data, sign); }
+void flups_do_mult(Solver* s, double* data, const FLUPS_SolverType type) { s->adv_mult(data, type); }
 
 void flups_pencilDirs(const FLUPS_BoundaryType* bc[3][2], int dirs[3]) {
     // flups.cpp:200-211: directions sorted (stably) by plan type

@@ -215,6 +215,14 @@ struct Solver {
     int timed_begin(const char* name, double bytes);
     void timed_end(int k);
     bool rot_split(int nbatch);
+    // ---------------------------------------------------------------- advanced API (flups.h:473-578)
+    size_t inner_elems = 0;               // doubles in the inner buffer
+    int64_t inner_pitch = 0;              // complex row pitch of the spectral layout
+    void ensure_inner();
+    void inner_spec_strides(int64_t str[3], int64_t& cstr) const;
+    void adv_copy(const Topology* topo, double* data, int sign);
+    void adv_fft(double* data, int sign);
+    void adv_mult(double* data, int type);
     void* spec_buf = nullptr;             // full spectrum of a split ROT solve
     size_t spec_bytes = 0;
     void collect_timing();

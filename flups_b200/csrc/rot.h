@@ -1,4 +1,4 @@
-// Pointwise curl-and-Green kernel of the ROT solve on the full spectrum (rot.cu).
+// Pointwise Green (STD) and curl-and-Green (ROT) multiplies on the full spectrum (rot.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -12,10 +12,13 @@ struct RotArgs {
     int n[3];            // extents (x fastest)
     int64_t str[3];      // element strides
     int64_t cstr;        // component stride
-    int nbatch;
-    MultSpec mult;       // mode 2 fields: Green, folds, wave-number tables, derivative order
+    int nbatch;          // ROT: groups of 3 components
+    int ncomp;           // STD: components multiplied
+    MultSpec mult;       // mode 1 (STD) or 2 (ROT): Green, folds, wave-number tables, derivative order
 };
 
 cudaError_t launch_rot_mult(const RotArgs& A, int f64, cudaStream_t s);
+// data in FP64 or the working precision, Green in the working precision
+cudaError_t launch_spec_mult(const RotArgs& A, int data_f64, int green_f64, cudaStream_t s);
 
 }  // namespace flb

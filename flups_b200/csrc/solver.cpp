@@ -1244,6 +1244,138 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
     else check_cuda(cudaGetLastError(), "solve");
 }
 
+// ---------------------------------------------------------------- advanced API
+// flups_get_innerBuffer / flups_get_innerTopo_* / flups_do_copy / do_FFT /
+// do_mult (Solver.cpp:518-530, 1281-1516).  The inner buffer is managed memory
+// (host code may fill and read it, as the reference's samples do; kernels read
+// it on the device) holding doubles in one of two layouts:
+//   physical: the user layout of flups_topo_new (x fastest, lda slowest);
+//   spectral: the full spectrum after every forward direction, complex,
+//             x fastest with rows padded to 8 complex (128 bytes), lda slowest;
+//             described by flups_get_innerTopo_spectral (axis 0, nf = 2).
+// The transforms run on the solver's work arrays; the first and last passes
+// read / write the doubles of the inner layouts.
+void Solver::ensure_inner() {
+    FLB_CHECK(is_setup, "flups_setup must be called before using the inner buffer");
+    const ArrState& S = st[ndim];
+    inner_pitch = ((int64_t)S.n[0] + 7) / 8 * 8;
+    const size_t spec = (size_t)inner_pitch * S.n[1] * S.n[2] * 2 * lda;
+    const size_t need = std::max(spec, topo_phys->memsize());
+    if (!inner || inner_elems < need) {
+        if (inner) cudaFree(inner);
+        inner = nullptr;
+        check_cuda(cudaMallocManaged(&inner, need * sizeof(double)), "inner buffer");
+        check_cuda(cudaMemset(inner, 0, need * sizeof(double)), "inner buffer");
+        inner_elems = need;
+    }
+    if (!topo_inner_phys) topo_inner_phys = new Topology(*topo_phys);
+    if (!topo_spec) {
+        topo_spec = new Topology(*topo_phys);
+        topo_spec->axis = 0;
+        topo_spec->nf = 2;
+        for (int d = 0; d < 3; ++d) {
+            topo_spec->nglob[d] = S.n[d];
+            topo_spec->nloc[d] = S.n[d];
+            topo_spec->nmem[d] = S.n[d];
+        }
+        topo_spec->nmem[0] = (int)inner_pitch;
+    }
+}
+
+void Solver::inner_spec_strides(int64_t str[3], int64_t& cstr) const {
+    const ArrState& S = st[ndim];
+    str[0] = 1;
+    str[1] = inner_pitch;
+    str[2] = inner_pitch * S.n[1];
+    cstr = inner_pitch * S.n[1] * S.n[2];
+}
+
+void Solver::adv_copy(const Topology* topo, double* data, int sign) {
+    FLB_CHECK(data != nullptr, "data is NULL");
+    FLB_CHECK(topo != nullptr && topo->lda == lda, "the solver lda = %d must match the topology one", lda);
+    FLB_CHECK(topo->memsize() == topo_phys->memsize(), "the topology must be the solver's physical topology");
+    ensure_inner();
+    const size_t bytes = topo->memsize() * sizeof(double);
+    if (sign == FLUPS_FORWARD)
+        check_cuda(cudaMemcpyAsync(inner, data, bytes, cudaMemcpyDefault, stream), "copy to the inner buffer");
+    else
+        check_cuda(cudaMemcpyAsync(data, inner, bytes, cudaMemcpyDefault, stream), "copy from the inner buffer");
+    check_cuda(cudaStreamSynchronize(stream), "copy");
+}
+
+void Solver::adv_fft(double* data, int sign) {
+    FLB_CHECK(data != nullptr, "data is NULL");
+    FLB_CHECK(sign == FLUPS_FORWARD || sign == FLUPS_BACKWARD || sign == FLUPS_BACKWARD_DIFF, "unknown sign %d", sign);
+    FLB_CHECK(sign != FLUPS_BACKWARD_DIFF || have_diff, "FLUPS_BACKWARD_DIFF needs a solver set up with a derivative order");
+    ensure_inner();
+    ensure_buffers(1);
+    const bool f64 = (precision == 64);
+    const int es = f64 ? 8 : 4;
+    pass_idx = 0;
+    if (sign == FLUPS_FORWARD) {
+        for (int ip = 0; ip < ndim; ++ip) {
+            const DirPlan& p = fwd[ip];
+            PassArgs A = base_pass(p.dim, st[ip], lda, lda);
+            A.st[0] = stage_forward(p, ip, f64);
+            if (ip == 0) {
+                set_strides_user(A.in_str, A.in_cstr);
+                A.in = data;
+            } else {
+                set_strides_internal(A.in_str, A.in_cstr, st[ip]);
+                A.in = buf[(ip - 1) % 2];
+            }
+            if (ip == ndim - 1) {
+                inner_spec_strides(A.out_str, A.out_cstr);
+                A.out = data;
+            } else {
+                set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
+                A.out = buf[ip % 2];
+            }
+            fit_lines(A, es);
+            run_pass(A, f64, ip == 0 ? true : f64, ip == ndim - 1 ? true : f64, "adv_fwd");
+        }
+    } else {
+        for (int ip = ndim - 1; ip >= 0; --ip) {
+            const DirPlan& p = (sign == FLUPS_BACKWARD_DIFF) ? dif[ip] : bwd[ip];
+            PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda, lda);
+            A.st[0] = stage_backward(p, fwd[ip], ip, f64);
+            if (ip == ndim - 1) {
+                inner_spec_strides(A.in_str, A.in_cstr);
+                A.in = data;
+            } else {
+                set_strides_internal(A.in_str, A.in_cstr, st[ip + 1]);
+                A.in = buf[ip % 2];
+            }
+            if (ip == 0) {
+                set_strides_user(A.out_str, A.out_cstr);
+                A.out = data;
+            } else {
+                set_strides_internal(A.out_str, A.out_cstr, st[ip]);
+                A.out = buf[(ip - 1) % 2];
+            }
+            fit_lines(A, es);
+            run_pass(A, f64, ip == ndim - 1 ? true : f64, ip == 0 ? true : f64, "adv_bwd");
+        }
+    }
+    check_cuda(cudaStreamSynchronize(stream), "flups_do_FFT");
+}
+
+void Solver::adv_mult(double* data, int type) {
+    FLB_CHECK(data != nullptr, "data is NULL");
+    FLB_CHECK(type == STD || (type == ROT && lda == 3 && odiff != NOD), "ROT needs lda = 3 and a derivative order");
+    ensure_inner();
+    RotArgs R;
+    memset(&R, 0, sizeof(R));
+    R.data = data;
+    for (int d = 0; d < 3; ++d) R.n[d] = st[ndim].n[d];
+    inner_spec_strides(R.str, R.cstr);
+    R.nbatch = 1;
+    R.ncomp = lda;
+    R.mult = mult_spec(type);
+    check_cuda(launch_spec_mult(R, 1, precision == 64 ? 1 : 0, stream), "flups_do_mult");
+    check_cuda(cudaStreamSynchronize(stream), "flups_do_mult");
+}
+
 // ---------------------------------------------------------------- autotuning
 std::string Solver::pass_key(const PassArgs& A, bool f64) const {
     char b[160];

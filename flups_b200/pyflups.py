@@ -114,6 +114,12 @@ def load_library(path=None):
         "flups_synchronize": (None, [vp]),
         "flups_b200_set_autotune": (None, [vp, c_int]),
         "flups_b200_set_col_tile": (None, [vp, c_int]),
+        "flups_get_innerBuffer": (vp, [vp]),
+        "flups_get_innerTopo_physical": (vp, [vp]),
+        "flups_get_innerTopo_spectral": (vp, [vp]),
+        "flups_do_copy": (None, [vp, vp, vp, c_int]),
+        "flups_do_FFT": (None, [vp, vp, c_int]),
+        "flups_do_mult": (None, [vp, vp, c_int]),
         "flups_solve_graph": (c_int, [vp, vp, vp, c_int, c_int]),
         "flups_get_last_error": (c_int, [vp]),
         "flups_get_device_bytes": (c_size_t, [vp, c_int]),
@@ -155,43 +161,51 @@ class Topology:
             _lib.flups_topo_free(self._topo)
             self._topo = None
 
+    @classmethod
+    def _borrowed(cls, ptr):
+        """A topology owned by a solver (flups_get_innerTopo_*): never freed here."""
+        t = cls.__new__(cls)
+        t._topo = None
+        t._view = ptr
+        return t
+
     @property
     def _ptr(self):
-        return self._topo
+        return self._topo if self._topo else getattr(self, "_view", None)
 
     @property
     def lda(self):
-        return _lib.flups_topo_get_lda(self._topo)
+        return _lib.flups_topo_get_lda(self._ptr)
 
     @property
     def axis(self):
-        return _lib.flups_topo_get_axis(self._topo)
+        return _lib.flups_topo_get_axis(self._ptr)
 
     def is_complex(self):
-        return bool(_lib.flups_topo_get_isComplex(self._topo))
+        return bool(_lib.flups_topo_get_isComplex(self._ptr))
 
     def get_nglob(self, dim):
-        return _lib.flups_topo_get_nglob(self._topo, dim)
+        return _lib.flups_topo_get_nglob(self._ptr, dim)
 
     def get_nloc(self, dim):
-        return _lib.flups_topo_get_nloc(self._topo, dim)
+        return _lib.flups_topo_get_nloc(self._ptr, dim)
 
     def get_nmem(self, dim):
-        return _lib.flups_topo_get_nmem(self._topo, dim)
+        return _lib.flups_topo_get_nmem(self._ptr, dim)
 
     def get_nproc(self, dim):
-        return _lib.flups_topo_get_nproc(self._topo, dim)
+        return _lib.flups_topo_get_nproc(self._ptr, dim)
 
     def get_istart(self):
         a = (c_int * 3)()
-        _lib.flups_topo_get_istartGlob(self._topo, a)
+        _lib.flups_topo_get_istartGlob(self._ptr, a)
         return np.array(a[:])
 
     def locsize(self):
-        return _lib.flups_topo_get_locsize(self._topo)
+        return _lib.flups_topo_get_locsize(self._ptr)
 
     def memsize(self):
-        return _lib.flups_topo_get_memsize(self._topo)
+        return _lib.flups_topo_get_memsize(self._ptr)
 
 
 class Profiler:
@@ -261,6 +275,30 @@ class Solver:
 
     def synchronize(self):
         _lib.flups_synchronize(self._solver)
+
+    # ---- advanced API (src/flups.h:473-578)
+    def get_inner_buffer(self):
+        """The solver's inner buffer (managed memory: host- and device-accessible)
+        as a numpy array of doubles, sized for both inner layouts."""
+        ptr = _lib.flups_get_innerBuffer(self._solver)
+        topo_s = self.get_inner_topo_spectral()
+        n = max(topo_s.memsize(), self._topology.memsize())
+        return np.ctypeslib.as_array((ctypes.c_double * n).from_address(ptr))
+
+    def get_inner_topo_physical(self):
+        return Topology._borrowed(_lib.flups_get_innerTopo_physical(self._solver))
+
+    def get_inner_topo_spectral(self):
+        return Topology._borrowed(_lib.flups_get_innerTopo_spectral(self._solver))
+
+    def do_copy(self, topology, data, sign):
+        _lib.flups_do_copy(self._solver, topology._ptr, _ptr(data), int(sign))
+
+    def do_fft(self, data, sign):
+        _lib.flups_do_FFT(self._solver, _ptr(data), int(sign))
+
+    def do_mult(self, data, solver_type=SolverType.STD):
+        _lib.flups_do_mult(self._solver, _ptr(data), int(solver_type))
 
     def set_autotune(self, on):
         _lib.flups_b200_set_autotune(self._solver, int(bool(on)))

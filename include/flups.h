@@ -6,7 +6,9 @@
  * cites the declaration it replaces.  The solver runs on one CUDA device with
  * a size-1 communicator.  Differences a caller can see:
  *   - rhs/field of flups_solve may be host or device pointers (detected per
- *     call); flups_get_innerBuffer returns a device pointer;
+ *     call); flups_get_innerBuffer returns CUDA managed memory (host code
+ *     and kernels may both use it) and the spectral inner topology is x
+ *     fastest (axis 0), complex, rows padded to 8 complex;
  *   - flups_set_stream takes a cudaStream_t (the reference ignores it);
  *   - programmer errors abort with a message, as FLUPS_CHECK does;
  *   - additive entry points (precision, batching, errors) live in
@@ -142,19 +144,22 @@ size_t flups_get_allocSize(FLUPS_Solver* s);
 void flups_get_spectralInfo(FLUPS_Solver* s, double kfact[3], double koffset[3], double symstart[3]);
 /* src/flups.h:494 */
 void flups_set_alpha(FLUPS_Solver* s, const double alpha);
-/* src/flups.h:509 -- device pointer to the solver's spectral buffer (doubles) */
+/* src/flups.h:509 -- the solver's inner buffer: managed memory (host and
+ * device), doubles, large enough for both inner layouts */
 double* flups_get_innerBuffer(FLUPS_Solver* s);
-/* src/flups.h:517 */
+/* src/flups.h:517 -- owned by the solver: the user layout (there are no pencils) */
 FLUPS_Topology* flups_get_innerTopo_physical(FLUPS_Solver* s);
-/* src/flups.h:525 */
+/* src/flups.h:525 -- owned by the solver: the full spectrum, axis 0, nf = 2 */
 FLUPS_Topology* flups_get_innerTopo_spectral(FLUPS_Solver* s);
-/* src/flups.h:534 */
+/* src/flups.h:534 -- accepted, no effect: the physical inner layout is the user's */
 void flups_skip_firstSwitchtopo(FLUPS_Solver* s);
 /* src/flups.h:544 -- host or device data in the physical topology <-> inner buffer */
 void flups_do_copy(FLUPS_Solver* s, const FLUPS_Topology* topo, double* data, const int sign);
-/* src/flups.h:552 -- data is the inner buffer (device) */
+/* src/flups.h:552 -- data is the inner buffer: FLUPS_FORWARD from the physical
+ * to the spectral layout, FLUPS_BACKWARD (or FLUPS_BACKWARD_DIFF after a ROT
+ * multiply) back; the unnormalised transforms of the reference */
 void flups_do_FFT(FLUPS_Solver* s, double* data, const int sign);
-/* src/flups.h:560 */
+/* src/flups.h:560 -- normfact * Green (STD) or normfact * Green * curl (ROT) */
 void flups_do_mult(FLUPS_Solver* s, double* data, const FLUPS_SolverType type);
 /* src/flups.h:570 */
 void flups_pencilDirs(const FLUPS_BoundaryType* bc[3][2], int dirs[3]);
