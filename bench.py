@@ -54,6 +54,7 @@ def parse():
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
+    ap.add_argument("--overlap", type=int, default=0, help="1: overlap the per-x-slab middle passes on three streams")
     return ap.parse_args()
 
 
@@ -559,6 +560,7 @@ def main():
     # ---------------------------------------------------------------- FP32 (headline)
     t32, s32, setup32 = make_solver(pf, n, args.kernel, 32, stream)
     s32.set_async(True)
+    s32.set_overlap(bool(args.overlap))
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
             s32.solve(field, rhs)

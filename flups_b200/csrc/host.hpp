@@ -228,6 +228,15 @@ struct Solver {
     void collect_timing();
     void check_cuda(cudaError_t e, const char* what);
     void do_fft_forward(const double* user_in, int nbatch);
+    void fwd_pass(int ip, const double* user_in, int nbatch);
+    void bwd_pass(int ip, double* user_out, int type, int nbatch);
+    // overlapped middle passes over x-slabs (flups_b200_set_overlap)
+    bool overlap = false;
+    static constexpr int kOvSlabs = 4;
+    cudaStream_t ov_stream[2] = {nullptr, nullptr};
+    cudaEvent_t ov_ev0 = nullptr, ov_evf[kOvSlabs] = {}, ov_evg[kOvSlabs] = {};
+    bool overlap_ok(int type) const;
+    void solve_overlap(const double* din, double* dout, int type, int nbatch);
     void do_fused(int type, int nbatch);
     void do_backward(double* user_out, int type, int nbatch);
     void do_fft_backward_fused(double* user_out, int type, int nbatch);

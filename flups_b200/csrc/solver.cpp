@@ -154,6 +154,17 @@ void Solver::dry_run(DirPlan p[3]) {
 
 Solver::~Solver() {
     drop_graphs();
+    if (ov_stream[0]) {
+        for (int i = 0; i < 2; ++i) {
+            cudaStreamSynchronize(ov_stream[i]);
+            cudaStreamDestroy(ov_stream[i]);
+        }
+        cudaEventDestroy(ov_ev0);
+        for (int k = 0; k < kOvSlabs; ++k) {
+            cudaEventDestroy(ov_evf[k]);
+            cudaEventDestroy(ov_evg[k]);
+        }
+    }
     if (capture_stream) cudaStreamDestroy(capture_stream);
     if (h2d_stream) {
         // copies of an async solve may still be in flight
@@ -586,6 +597,10 @@ void Solver::restrict_slab(PassArgs& A, bool in_f64, bool out_f64) const {
     const int a = (A.axis == 0) ? 1 : 0;
     const int d = slab_dim;
     const int64_t lo = slab_lo;
+    if (A.fused) {
+        // the folded Green's function is not folded along d: shift it with the slab
+        A.mult.green = (const char*)A.mult.green + lo * A.mult.gstr[d] * (precision == 64 ? 8 : 4);
+    }
     const int64_t ein = (in_f64 ? 8 : 4) * (A.st[0].in_cplx ? 2 : 1);
     const int64_t eout = (out_f64 ? 8 : 4) * (A.st[A.fused ? 1 : 0].out_cplx ? 2 : 1);
     A.in = (const char*)A.in + lo * A.in_str[d] * ein;
@@ -597,7 +612,8 @@ void Solver::restrict_slab(PassArgs& A, bool in_f64, bool out_f64) const {
 
 void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, const char* name) {
     PassArgs A = Ain;
-    if (slab_dim >= 0 && !A.fused && A.axis != slab_dim) restrict_slab(A, in_f64, out_f64);
+    if (slab_dim >= 0 && A.axis != slab_dim && (!A.fused || (A.mult.mode == 1 && A.mult.gfold[slab_dim] == 0)))
+        restrict_slab(A, in_f64, out_f64);
     const int fk = fast_kind(A, f64, in_f64, out_f64);
     if (dry) {
         dry_passes.push_back(A);
@@ -967,25 +983,27 @@ static bool is_device_ptr(const void* p) {
 }
 
 void Solver::do_fft_forward(const double* user_in, int nbatch) {
+    for (int ip = 0; ip < ndim - 1; ++ip) fwd_pass(ip, user_in, nbatch);
+}
+
+void Solver::fwd_pass(int ip, const double* user_in, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
-    for (int ip = 0; ip < ndim - 1; ++ip) {
-        const DirPlan& p = fwd[ip];
-        PassArgs A = base_pass(p.dim, st[ip], lda * nbatch, lda);
-        A.st[0] = stage_forward(p, ip, f64);
-        if (ip == 0) {
-            set_strides_user(A.in_str, A.in_cstr);
-            A.in = user_in;
-        } else {
-            set_strides_internal(A.in_str, A.in_cstr, st[ip]);
-            A.in = buf[(ip - 1) % 2];
-        }
-        set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
-        A.out = buf[ip % 2];
-        fit_lines(A, es);
-        static const char* fn[3] = {"fwd0", "fwd1", "fwd2"};
-        run_pass(A, f64, ip == 0 ? true : f64, f64, fn[ip]);
+    const DirPlan& p = fwd[ip];
+    PassArgs A = base_pass(p.dim, st[ip], lda * nbatch, lda);
+    A.st[0] = stage_forward(p, ip, f64);
+    if (ip == 0) {
+        set_strides_user(A.in_str, A.in_cstr);
+        A.in = user_in;
+    } else {
+        set_strides_internal(A.in_str, A.in_cstr, st[ip]);
+        A.in = buf[(ip - 1) % 2];
     }
+    set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
+    A.out = buf[ip % 2];
+    fit_lines(A, es);
+    static const char* fn[3] = {"fwd0", "fwd1", "fwd2"};
+    run_pass(A, f64, ip == 0 ? true : f64, f64, fn[ip]);
 }
 
 void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
@@ -1086,25 +1104,77 @@ void Solver::do_fused(int type, int nbatch) {
 }
 
 void Solver::do_backward(double* user_out, int type, int nbatch) {
+    for (int ip = ndim - 2; ip >= 0; --ip) bwd_pass(ip, user_out, type, nbatch);
+}
+
+void Solver::bwd_pass(int ip, double* user_out, int type, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
-    for (int ip = ndim - 2; ip >= 0; --ip) {
-        const DirPlan& p = (type == ROT) ? dif[ip] : bwd[ip];
-        PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda * nbatch, lda);
-        A.st[0] = stage_backward(p, fwd[ip], ip, f64);
-        set_strides_internal(A.in_str, A.in_cstr, st[ip + 1]);
-        A.in = buf[ip % 2];
-        if (ip == 0) {
-            set_strides_user(A.out_str, A.out_cstr);
-            A.out = user_out;
-        } else {
-            set_strides_internal(A.out_str, A.out_cstr, st[ip]);
-            A.out = buf[(ip - 1) % 2];
-        }
-        fit_lines(A, es);
-        static const char* bn[3] = {"bwd0", "bwd1", "bwd2"};
-        run_pass(A, f64, f64, ip == 0 ? true : f64, bn[ip]);
+    const DirPlan& p = (type == ROT) ? dif[ip] : bwd[ip];
+    PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda * nbatch, lda);
+    A.st[0] = stage_backward(p, fwd[ip], ip, f64);
+    set_strides_internal(A.in_str, A.in_cstr, st[ip + 1]);
+    A.in = buf[ip % 2];
+    if (ip == 0) {
+        set_strides_user(A.out_str, A.out_cstr);
+        A.out = user_out;
+    } else {
+        set_strides_internal(A.out_str, A.out_cstr, st[ip]);
+        A.out = buf[(ip - 1) % 2];
     }
+    fit_lines(A, es);
+    static const char* bn[3] = {"bwd0", "bwd1", "bwd2"};
+    run_pass(A, f64, f64, ip == 0 ? true : f64, bn[ip]);
+}
+
+// Overlapped middle passes (STD, x transformed first, device arrays): after
+// the x pass, the y forward, fused z and y inverse passes of an x-slab only
+// touch that slab, so slab k's fused pass (issue-bound) runs on one stream
+// while slab k+1's y forward and slab k-1's y inverse (memory-bound) run on
+// others; the x inverse pass waits for every slab.
+bool Solver::overlap_ok(int type) const {
+    return overlap && !timing && !dry && !capturing && ndim == 3 && type == STD && fwd[0].dim == 0 && slab_dim < 0 &&
+           gfold_M[0] == 0 && st[1].n[0] >= 64;
+}
+
+void Solver::solve_overlap(const double* din, double* dout, int type, int nbatch) {
+    if (!ov_stream[0]) {
+        for (int i = 0; i < 2; ++i) check_cuda(cudaStreamCreateWithFlags(&ov_stream[i], cudaStreamNonBlocking), "stream");
+        check_cuda(cudaEventCreateWithFlags(&ov_ev0, cudaEventDisableTiming), "event");
+        for (int k = 0; k < kOvSlabs; ++k) {
+            check_cuda(cudaEventCreateWithFlags(&ov_evf[k], cudaEventDisableTiming), "event");
+            check_cuda(cudaEventCreateWithFlags(&ov_evg[k], cudaEventDisableTiming), "event");
+        }
+    }
+    pass_idx = 0;
+    fwd_pass(0, din, nbatch);
+    check_cuda(cudaEventRecord(ov_ev0, stream), "event record");
+    const cudaStream_t main = stream;
+    const int nx = st[1].n[0];
+    // slab bounds on 32-column boundaries (whole CTA tiles, 128-byte Green rows)
+    const int chunks = (nx + 31) / 32;
+    const int ns = std::min(kOvSlabs, chunks);
+    for (int k = 0; k < ns; ++k) {
+        const int lo = std::min(nx, (int)((int64_t)k * chunks / ns) * 32);
+        const int hi = (k == ns - 1) ? nx : std::min(nx, (int)((int64_t)(k + 1) * chunks / ns) * 32);
+        slab_dim = 0;
+        slab_lo = lo;
+        slab_hi = hi;
+        stream = ov_stream[0];
+        if (k == 0) check_cuda(cudaStreamWaitEvent(stream, ov_ev0, 0), "stream wait");
+        fwd_pass(1, nullptr, nbatch);
+        check_cuda(cudaEventRecord(ov_evf[k], stream), "event record");
+        stream = ov_stream[1];
+        check_cuda(cudaStreamWaitEvent(stream, ov_evf[k], 0), "stream wait");
+        do_fused(type, nbatch);
+        check_cuda(cudaEventRecord(ov_evg[k], stream), "event record");
+        stream = main;
+        check_cuda(cudaStreamWaitEvent(stream, ov_evg[k], 0), "stream wait");
+        bwd_pass(1, nullptr, type, nbatch);
+    }
+    slab_dim = -1;
+    stream = main;
+    bwd_pass(0, dout, type, nbatch);
 }
 
 void Solver::solve(double* field, double* rhs, int type, int nbatch) {
@@ -1140,8 +1210,12 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     }
     if (!dev_out) dout = stage_in;
     pass_idx = 0;
-    do_fft_forward(din, nbatch);
-    do_fft_backward_fused(dout, type, nbatch);
+    if (dev_in && dev_out && overlap_ok(type)) {
+        solve_overlap(din, dout, type, nbatch);
+    } else {
+        do_fft_forward(din, nbatch);
+        do_fft_backward_fused(dout, type, nbatch);
+    }
     collect_timing();
     if (!dev_out) {
         check_cuda(cudaMemcpyAsync(field, dout, user_elems * sizeof(double), cudaMemcpyDeviceToHost, stream), "field download");

@@ -114,6 +114,7 @@ def load_library(path=None):
         "flups_synchronize": (None, [vp]),
         "flups_b200_set_autotune": (None, [vp, c_int]),
         "flups_b200_set_col_tile": (None, [vp, c_int]),
+        "flups_b200_set_overlap": (None, [vp, c_int]),
         "flups_get_innerBuffer": (vp, [vp]),
         "flups_get_innerTopo_physical": (vp, [vp]),
         "flups_get_innerTopo_spectral": (vp, [vp]),
@@ -302,6 +303,10 @@ class Solver:
 
     def set_autotune(self, on):
         _lib.flups_b200_set_autotune(self._solver, int(bool(on)))
+
+    def set_overlap(self, on):
+        """Overlap the per-x-slab middle passes on three streams (device arrays, STD)."""
+        _lib.flups_b200_set_overlap(self._solver, int(bool(on)))
 
     def set_col_tile(self, tile):
         """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""

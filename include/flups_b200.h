@@ -81,6 +81,13 @@ void flups_b200_set_fast_kernels(struct Solver* s, int on);
  * that first call synchronises the stream.  No reference counterpart. */
 void flups_b200_set_autotune(struct Solver* s, int on);
 
+/* Overlap the middle passes of a solve of device arrays (1 = on, default 0):
+ * after the x transform, the y forward, fused z and y inverse passes run per
+ * x-slab on three streams, so one slab's fused pass (bound by arithmetic)
+ * runs beside other slabs' y passes (bound by memory).  Results are
+ * identical.  No reference counterpart. */
+void flups_b200_set_overlap(struct Solver* s, int on);
+
 /* Force the CTA tile of every column pass: 0 = default or tuned, 1 = 256
  * threads, 2 = 128 threads.  For cross-checking the tiles. */
 void flups_b200_set_col_tile(struct Solver* s, int tile);

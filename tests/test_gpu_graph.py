@@ -68,3 +68,22 @@ def test_graph_and_autotune_match_plain_batch(precision):
     torch.cuda.synchronize()
     assert torch.equal(out, ref2)
     assert s.last_error() == 0
+
+
+@pytest.mark.parametrize("n,precision", [(64, 64), (128, 32), (200, 32)])
+def test_overlapped_middle_passes_bitwise(n, precision):
+    """The x-slab overlap of the y / fused z / y passes on three streams gives
+    the plain solve's result bit for bit."""
+    import torch
+    t, s = _setup(n, LGF_2, precision)
+    rhs = torch.from_numpy(_rhs(n, 1, 6)).cuda()
+    ref = torch.zeros_like(rhs)
+    s.solve(ref, rhs)
+    torch.cuda.synchronize()
+    s.set_overlap(True)
+    out = torch.full_like(rhs, float("nan"))
+    for _ in range(2):
+        s.solve(out, rhs)
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+    assert s.last_error() == 0
