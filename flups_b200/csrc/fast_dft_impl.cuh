@@ -86,7 +86,10 @@ struct RegFFT {
     // the later-stage table is staged in shared memory when it is small
     // (FP32 lines up to 1024: one later stage, at most 8 KB)
     static constexpr int TWN = stage_table_entries(L, R1);
-    static constexpr bool TWS = TWN > 0 && TWN * (int)sizeof(C) <= 8192;
+#ifndef FLB_TW_SMEM_MAX
+#define FLB_TW_SMEM_MAX 8192
+#endif
+    static constexpr bool TWS = TWN > 0 && TWN * (int)sizeof(C) <= FLB_TW_SMEM_MAX;
     static constexpr int TW_SMEM = TWS ? TWN : 0;  // complex entries of shared memory for the table
     // line stride in shared memory (complex elements): the swizzled length rounded
     // to 16, plus an offset that puts the lines met by one half-warp on distinct
@@ -284,9 +287,12 @@ __device__ __forceinline__ void stage_green(const ColArgs& a, T* gs, int o) {
 #ifndef FLB_COL_THREADS_PER_SM
 #define FLB_COL_THREADS_PER_SM 512
 #endif
-template <int THREADS>
+#ifndef FLB_FUSED_THREADS_PER_SM
+#define FLB_FUSED_THREADS_PER_SM 512
+#endif
+template <int THREADS, bool FUSED = false>
 struct Occ {
-    static constexpr int want = FLB_COL_THREADS_PER_SM / (THREADS < 64 ? 64 : THREADS);
+    static constexpr int want = (FUSED ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM) / (THREADS < 64 ? 64 : THREADS);
     static constexpr int blocks = want < 1 ? 1 : want;
 };
 
@@ -298,7 +304,7 @@ enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
 //      2: forward, Green multiply, inverse (SH: loaded and stored part).
 // The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
 template <typename T, int L, int R1, int TX, int MODE, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), Occ<TX * (L / R1)>::blocks) col_dft_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2>::blocks)) col_dft_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
