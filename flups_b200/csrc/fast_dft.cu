@@ -9,14 +9,14 @@ namespace flb {
 bool fast_col_supported(int L) {
     switch (L) {
         case 64: case 128: case 256: case 512: case 1024: case 2048:
-        case 96: case 192: case 384: case 768: case 1536: return true;
+        case 48: case 96: case 192: case 384: case 768: case 1536: return true;
     }
     return false;
 }
 bool fast_row_supported(int L) {
     switch (L) {
-        case 128: case 256: case 512: case 1024: case 2048: case 4096:
-        case 96: case 192: case 384: case 768: case 1536: case 3072: return true;
+        case 64: case 128: case 256: case 512: case 1024: case 2048: case 4096:
+        case 48: case 96: case 192: case 384: case 768: case 1536: case 3072: return true;
     }
     return false;
 }
@@ -34,6 +34,25 @@ cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncom
     if (f64) return (mode == 2) ? launch_col_f64_m2(sh, L, a, ncomp, s) : launch_col_f64_m01(mode, sh, L, a, ncomp, s);
     if (mode == 2) return launch_col_f32_m2(sh, L, a, ncomp, s);
     return launch_col_f32_m01(mode, sh, L, a, ncomp, s);
+}
+
+bool fast_r2r_supported(int M) {
+    switch (M) {
+        case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 2048: return true;
+    }
+    return false;
+}
+
+cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s) {
+    return launch_r2r_units(f64, a.in_f64, a.out_f64, M, a, ncomp, s);
+}
+
+cudaError_t launch_fast_colreal(int f64, int c2r, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };
+    // the periodic copy's extra element is stored apart
+    const int sh = c2r ? shape(a.period >= 0 ? a.nout - 1 : a.nout) : shape(a.nin > L ? L : a.nin);
+    if (f64) return launch_colreal_f64(c2r, sh, L, a, ncomp, s);
+    return launch_colreal_f32(c2r, sh, L, a, ncomp, s);
 }
 
 // the real side (r2c input / c2r output) is the user's doubles or the working precision

@@ -21,6 +21,7 @@ struct ColArgs {
     int f_x, f_line, f_outer;              // fold lengths (0 = none)
     double normfact;
     int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
+    int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
 };
 
 enum { COL_TILE_DEFAULT = 0, COL_TILE_256 = 1, COL_TILE_128 = 2 };
@@ -37,6 +38,12 @@ struct RowArgs {
     int in_f64, out_f64;
     const void* tw;         // W_L^q, q < L (L = 2 * Lh): the real-to-half-length split
     const void* tws;        // later-stage twiddle table of the Lh-point DFT (fast_stage_table)
+    // r2r rows (DCT / DST I-IV through an M-point complex DFT of the extended row)
+    int kind;               // LineKind of the transform
+    int n;                  // FFTW size n_in
+    int nstore;             // outputs written (before post-processing)
+    int postpro, nfftw;     // PostPro bits and the index PP_ENFORCE_PERIOD copies from 0
+    const void* tw2;        // W_{2M}^q, q < 2M (pre/post twiddles of the r2r kinds)
 };
 
 bool fast_col_supported(int L);
@@ -74,5 +81,10 @@ __host__ __device__ inline void fast_stage_exponent(int n, int r1, int e, int* q
 
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
+// r2r rows (DCT / DST I-IV) through an M-point complex register DFT
+bool fast_r2r_supported(int M);
+cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
+// column r2c (c2r = 0: real in, X[0..L/2] out) and c2r (c2r = 1)
+cudaError_t launch_fast_colreal(int f64, int c2r, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 
 }  // namespace flb

@@ -374,6 +374,82 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2>:
     }
 }
 
+// ---------------------------------------------------------------- columns, real side
+// r2c (C2R = false): real column of nin values (zero beyond) -> X[0..L/2];
+// SH: loaded part.  c2r (C2R = true): X[0..L/2] -> real column, the upper half
+// of the spectrum read as conj(X[L-k]) straight from memory (no exchange);
+// SH: stored part.  Im X[0] and Im X[L/2] do not enter a real result.
+template <typename T, int L, int R1, int TX, bool C2R, int SH>
+__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) col_real_kernel(const ColArgs a) {
+    using F = RegFFT<T, L, R1>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int c = threadIdx.x % TX, p = threadIdx.x / TX;
+    const int x = blockIdx.x * TX + c;
+    const int o = blockIdx.y;
+    const int comp = blockIdx.z;
+    const bool valid = x < a.nx;
+    const C* tws = stage_twiddles<F>(a.tws, sm + TX * F::SC);
+    C v[R1];
+    if constexpr (!C2R) {
+        constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;
+        const T* in = valid ? reinterpret_cast<const T*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+                            : reinterpret_cast<const T*>(a.in);
+        const int ls = valid ? P * (int)a.in_lstr : 0;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            if (r >= NLD) {
+                v[r] = mkc((T)0, (T)0);
+            } else {
+                const bool ok = valid && (SH != SH_ANY || p + P * r < a.nin);
+                const T t = in[ok ? r * ls : 0];
+                v[r] = mkc(ok ? t : (T)0, (T)0);
+            }
+        }
+    } else {
+        // X[k] for k <= L/2 (r < R1/2, and r = R1/2 on p = 0); conj X[L-k] above
+        const C* base = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x
+                              : reinterpret_cast<const C*>(a.in);
+        const int lstr = valid ? (int)a.in_lstr : 0;
+        const C* lo = base + (int64_t)p * lstr;
+        const C* hi = base + (int64_t)(L - p) * lstr;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            C t;
+            if (r < R1 / 2) t = lo[r * P * lstr];
+            else t = cconj(hi[-r * P * lstr]);  // k = L/2 (r = R1/2, p = 0): conj X[L/2], imaginary part dropped below
+            if (r == 0 && p == 0) t.y = (T)0;
+            if (r == R1 / 2 && p == 0) t.y = (T)0;
+            v[r] = valid ? t : mkc((T)0, (T)0);
+        }
+    }
+    if constexpr (F::TWS) cp_async_wait<0>();
+    C* line = sm + c * F::SC;
+    if constexpr (C2R) F::template fft<false, true>(v, line, p, tws);
+    else F::template fft<SH == SH_HALF, false>(v, line, p, tws);
+    if (!valid) return;
+    if constexpr (!C2R) {
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int os = P * (int)a.out_lstr;
+#pragma unroll
+        for (int r = 0; r <= R1 / 2; ++r) {
+            if (r < R1 / 2 || p == 0) out[r * os] = v[r];
+        }
+        if (p == 0 && a.period >= 0) out[(int64_t)a.period * a.out_lstr] = v[0];
+    } else {
+        constexpr int NST = (SH == SH_HALF) ? R1 / 2 : R1;
+        T* out = reinterpret_cast<T*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int os = P * (int)a.out_lstr;
+#pragma unroll
+        for (int r = 0; r < NST; ++r) {
+            if (SH != SH_ANY || p + P * r < a.nout) out[r * os] = v[r].x;
+        }
+        if (p == 0 && a.period >= 0) out[(int64_t)a.period * a.out_lstr] = v[0].x;
+    }
+}
+
 // ---------------------------------------------------------------- rows: r2c
 template <typename IT> struct Vec2;
 template <> struct Vec2<float> { using V = float2; };
@@ -445,6 +521,117 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
             const C z0 = line[0];
             dst[LH] = mkc(z0.x - z0.y, (T)0);
         }
+    }
+}
+
+// ---------------------------------------------------------------- rows: r2r
+// DCT / DST I-IV of real rows through the M-point complex DFT of the extended
+// row (the general line pass's formulas, csrc/line_pass.cu): the raw row is
+// staged in shared memory, c[m] is built from it (reflections, pre-twiddles),
+// one forward register DFT, C is exchanged through shared memory for the
+// shifted reads of the odd kinds, and Y_k (post-twiddles, post-processing) is
+// stored.  IT / OT: types of the real input / output (user doubles or the
+// working precision).
+template <typename T, typename IT, typename OT, int M, int R1, int TR>
+__global__ void __launch_bounds__(TR * (M / R1), (Occ<TR * (M / R1)>::blocks)) row_r2r_kernel(const RowArgs a) {
+    using F = RegFFT<T, M, R1, true>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int p = threadIdx.x % P, rr = threadIdx.x / P;
+    const int row = blockIdx.x * TR + rr;
+    const int comp = blockIdx.y;
+    const bool valid = row < a.nrows;
+    const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
+    const IT* src = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
+    C* line = sm + rr * F::SC;
+    const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
+    const C* tw = reinterpret_cast<const C*>(a.tw2);
+    const int n = a.n, kind = a.kind, nsrc = a.nin;
+    const T z = (T)0;
+    // raw row in shared memory (zero beyond the source)
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        const int j = p + P * r;
+        const IT u = (valid && j < nsrc) ? src[j] : (IT)0;
+        line[F::sw(j)] = mkc((T)u, z);
+    }
+    if constexpr (F::TWS) cp_async_wait<0>();
+    __syncthreads();
+    auto u = [&](int t) { return line[F::sw(t)].x; };
+    C v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        const int m = p + P * r;
+        T x;
+        C c = mkc(z, z);
+        switch (kind) {
+            case LK_DCT1: c = mkc(m < n ? u(m) : u(M - m), z); break;
+            case LK_DST1:
+                if (m != 0 && m != n + 1) c = mkc(m <= n ? u(m - 1) : -u(M - m - 1), z);
+                break;
+            case LK_DCT2: c = mkc(m < n ? u(m) : u(2 * n - 1 - m), z); break;
+            case LK_DST2: c = mkc(m < n ? u(m) : -u(2 * n - 1 - m), z); break;
+            case LK_DCT3:
+                if (m < n) {
+                    x = (m == 0 ? (T)1 : (T)2) * u(m);
+                    const C w = tw[m];
+                    c = mkc(w.x * x, w.y * x);
+                }
+                break;
+            case LK_DST3:
+                if (m != 0 && m <= n) {
+                    x = (m - 1 == n - 1 ? (T)1 : (T)2) * u(m - 1);
+                    const C w = tw[m];
+                    c = mkc(w.x * x, w.y * x);
+                }
+                break;
+            default:  // DCT4, DST4
+                if (m < n) {
+                    x = u(m);
+                    const C w = tw[m];
+                    c = mkc(w.x * x, w.y * x);
+                }
+                break;
+        }
+        v[r] = c;
+    }
+    F::template fft<false, false>(v, line, p, tws);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    __syncthreads();
+    if (!valid) return;
+    OT* dst = reinterpret_cast<OT*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2;
+    // e^{-i pi / (4n)} of the type-IV kinds
+    double ps, pc;
+    sincospi(-0.25 / (double)n, &ps, &pc);
+    const C ph4 = mkc((T)pc, (T)ps);
+    const bool first = a.postpro & PP_NULL_FIRST, last = a.postpro & PP_NULL_LAST, period = a.postpro & PP_ENFORCE_PERIOD;
+    auto value = [&](int k) -> T {
+        if (k >= n) return (k < nsrc) ? (T)src[k] : z;  // beyond the transform: the padded input stays
+        switch (kind) {
+            case LK_DCT1: return line[F::sw(k)].x;
+            case LK_DST1: return -line[F::sw(k + 1)].y;
+            case LK_DCT2: return cmul(tw[k], line[F::sw(k)]).x;
+            case LK_DST2: return -cmul(tw[k + 1], line[F::sw(k + 1)]).y;
+            case LK_DCT3: return line[F::sw(k)].x;
+            case LK_DST3: return -line[F::sw(k)].y;
+            case LK_DCT4: return (T)2 * cmul(ph4, cmul(tw[k], line[F::sw(k)])).x;
+            default: return -(T)2 * cmul(ph4, cmul(tw[k], line[F::sw(k)])).y;
+        }
+    };
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        const int i = p + P * r;
+        if (i >= a.nstore) continue;
+        T y;
+        if (first && i == 0) y = z;
+        else if (last && i == a.nstore - 1) y = z;
+        else if (period && !first && !last && i == a.nfftw) y = value(0);
+        else y = value(i);
+        dst[i] = (OT)y;
     }
 }
 
@@ -526,6 +713,9 @@ cudaError_t launch_col_f32_m2(int sh, int L, const ColArgs& a, int ncomp, cudaSt
 cudaError_t launch_col_f64_m01(int mode, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f64_m2(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_row_units(int f64, int c2r, int xt64, bool half, int L, const RowArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_r2r_units(int f64, int in64, int out64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_colreal_f64(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 
 template <typename T, int L, int R1, int TX, int MODE, int SH>
 inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
@@ -572,6 +762,7 @@ inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStrea
         case 512: return wide ? launch_col_threads<T, 512, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 512, 128, MODE, SH>(a, ncomp, s);
         case 1024: return wide ? launch_col_threads<T, 1024, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 1024, 128, MODE, SH>(a, ncomp, s);
         case 2048: return wide ? launch_col_threads<T, 2048, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 2048, 128, MODE, SH>(a, ncomp, s);
+        case 48: return wide ? launch_col_threads<T, 48, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 48, 128, MODE, SH>(a, ncomp, s);
         case 96: return wide ? launch_col_threads<T, 96, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 96, 128, MODE, SH>(a, ncomp, s);
         case 192: return wide ? launch_col_threads<T, 192, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 192, 128, MODE, SH>(a, ncomp, s);
         case 384: return wide ? launch_col_threads<T, 384, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 384, 128, MODE, SH>(a, ncomp, s);
@@ -581,11 +772,89 @@ inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStrea
     return cudaErrorInvalidValue;
 }
 
+template <typename T, int L, bool C2R, int SH>
+inline cudaError_t launch_colreal_t(const ColArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int R1 = fast_radix1_of(L, sizeof(T) == 8);
+    constexpr int TX = (L == 512 ? 128 : 256) / (L / R1);
+    static_assert(TX >= 1, "tile narrower than one column");
+    using F = RegFFT<T, L, R1>;
+    const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(col_real_kernel<T, L, R1, TX, C2R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
+    col_real_kernel<T, L, R1, TX, C2R, SH><<<grid, TX * F::P, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T, bool C2R, int SH>
+inline cudaError_t launch_colreal_len(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    switch (L) {
+        case 48: return launch_colreal_t<T, 48, C2R, SH>(a, ncomp, s);
+        case 64: return launch_colreal_t<T, 64, C2R, SH>(a, ncomp, s);
+        case 96: return launch_colreal_t<T, 96, C2R, SH>(a, ncomp, s);
+        case 128: return launch_colreal_t<T, 128, C2R, SH>(a, ncomp, s);
+        case 192: return launch_colreal_t<T, 192, C2R, SH>(a, ncomp, s);
+        case 256: return launch_colreal_t<T, 256, C2R, SH>(a, ncomp, s);
+        case 384: return launch_colreal_t<T, 384, C2R, SH>(a, ncomp, s);
+        case 512: return launch_colreal_t<T, 512, C2R, SH>(a, ncomp, s);
+        case 768: return launch_colreal_t<T, 768, C2R, SH>(a, ncomp, s);
+        case 1024: return launch_colreal_t<T, 1024, C2R, SH>(a, ncomp, s);
+        case 1536: return launch_colreal_t<T, 1536, C2R, SH>(a, ncomp, s);
+        case 2048: return launch_colreal_t<T, 2048, C2R, SH>(a, ncomp, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T, bool C2R>
+inline cudaError_t launch_colreal_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    if (sh == SH_FULL) return launch_colreal_len<T, C2R, SH_FULL>(L, a, ncomp, s);
+    if (sh == SH_HALF) return launch_colreal_len<T, C2R, SH_HALF>(L, a, ncomp, s);
+    return launch_colreal_len<T, C2R, SH_ANY>(L, a, ncomp, s);
+}
+
 template <typename T, int MODE>
 inline cudaError_t launch_col_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     if (sh == SH_FULL) return launch_col_mode<T, MODE, SH_FULL>(L, a, ncomp, s);
     if (sh == SH_HALF) return launch_col_mode<T, MODE, SH_HALF>(L, a, ncomp, s);
     return launch_col_mode<T, MODE, SH_ANY>(L, a, ncomp, s);
+}
+
+template <typename T, typename IT, typename OT, int M>
+inline cudaError_t launch_r2r_t(const RowArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int R1 = fast_radix1_of(M, sizeof(T) == 8);
+    using F = RegFFT<T, M, R1, true>;
+    constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
+    const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(row_r2r_kernel<T, IT, OT, M, R1, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((a.nrows + TR - 1) / TR, ncomp);
+    row_r2r_kernel<T, IT, OT, M, R1, TR><<<grid, TR * F::P, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T, typename IT, typename OT>
+inline cudaError_t launch_r2r_len(int M, const RowArgs& a, int ncomp, cudaStream_t s) {
+    switch (M) {
+        case 64: return launch_r2r_t<T, IT, OT, 64>(a, ncomp, s);
+        case 96: return launch_r2r_t<T, IT, OT, 96>(a, ncomp, s);
+        case 128: return launch_r2r_t<T, IT, OT, 128>(a, ncomp, s);
+        case 192: return launch_r2r_t<T, IT, OT, 192>(a, ncomp, s);
+        case 256: return launch_r2r_t<T, IT, OT, 256>(a, ncomp, s);
+        case 384: return launch_r2r_t<T, IT, OT, 384>(a, ncomp, s);
+        case 512: return launch_r2r_t<T, IT, OT, 512>(a, ncomp, s);
+        case 768: return launch_r2r_t<T, IT, OT, 768>(a, ncomp, s);
+        case 1024: return launch_r2r_t<T, IT, OT, 1024>(a, ncomp, s);
+        case 2048: return launch_r2r_t<T, IT, OT, 2048>(a, ncomp, s);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
@@ -619,6 +888,8 @@ inline cudaError_t launch_row_len(int L, const RowArgs& a, int ncomp, cudaStream
         case 1024: return launch_row_t<T, XT, 512, fast_radix1_of(512, F64), C2R, HALF>(a, ncomp, s);
         case 2048: return launch_row_t<T, XT, 1024, fast_radix1_of(1024, F64), C2R, HALF>(a, ncomp, s);
         case 4096: return launch_row_t<T, XT, 2048, fast_radix1_of(2048, F64), C2R, HALF>(a, ncomp, s);
+        case 48: return launch_row_t<T, XT, 24, fast_radix1_of(24, F64), C2R, HALF>(a, ncomp, s);
+        case 64: return launch_row_t<T, XT, 32, fast_radix1_of(32, F64), C2R, HALF>(a, ncomp, s);
         case 96: return launch_row_t<T, XT, 48, fast_radix1_of(48, F64), C2R, HALF>(a, ncomp, s);
         case 192: return launch_row_t<T, XT, 96, fast_radix1_of(96, F64), C2R, HALF>(a, ncomp, s);
         case 384: return launch_row_t<T, XT, 192, fast_radix1_of(192, F64), C2R, HALF>(a, ncomp, s);

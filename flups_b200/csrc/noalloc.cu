@@ -153,7 +153,10 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
         kinds[i] = s->fast_kind(A, f64, in64, out64);
         if (kinds[i] == 0) {
             for (int sg = 0; sg <= A.fused; ++sg) slot_for(2 * A.st[sg].M, 0);
-        } else if (kinds[i] == 1) {
+        } else if (kinds[i] == 1 || kinds[i] == 3) {
+            slot_for(A.st[0].M, 1);
+        } else if (kinds[i] == 4) {
+            slot_for(2 * A.st[0].M, 0);
             slot_for(A.st[0].M, 1);
         } else {
             slot_for(A.st[0].M, 0);
@@ -189,6 +192,13 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             if (kinds[i] == 1) {
                 c.tws = tw_of(L, 1);
                 e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
+            } else if (kinds[i] == 3) {
+                c.tws = tw_of(L, 1);
+                e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
+            } else if (kinds[i] == 4) {
+                r.tw2 = tw_of(2 * L, 0);
+                r.tws = tw_of(L, 1);
+                e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
             } else {
                 r.tw = tw_of(L, 0);
                 r.tws = tw_of(L / 2, 1);

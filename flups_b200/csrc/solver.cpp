@@ -423,6 +423,51 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
     // vector loads/stores of complex (or real pairs) need their natural alignment
     const uintptr_t ain = dry ? 0 : (uintptr_t)A.in, aout = dry ? 0 : (uintptr_t)A.out;
     if ((ain % (in_f64 ? 16 : 8)) != 0 || (aout % (out_f64 ? 16 : 8)) != 0) return 0;
+    {
+        const LineStage& S0 = A.st[0];
+        const int k0 = S0.spec[0].kind;
+        if (A.axis != 0 && !A.fused && (k0 == LK_R2C || k0 == LK_C2R)) {
+            // columns of a real transform (r2c forward, c2r backward), working precision;
+            // the node-centred periodic copy (PP_ENFORCE_PERIOD of index nfftw from 0) in the kernel
+            const int L = S0.M;
+            const LineSpec& sp0 = S0.spec[0];
+            for (int c = 0; c < A.lda; ++c) {
+                const LineSpec& sp = S0.spec[c];
+                if (sp.kind != k0 || sp.n_in != sp0.n_in || sp.fi != 0 || sp.fo != 0 || sp.postpro != sp0.postpro ||
+                    sp.nfftw != sp0.nfftw)
+                    return 0;
+            }
+            if (sp0.postpro != PP_NONE && sp0.postpro != PP_ENFORCE_PERIOD) return 0;
+            const int extra = (sp0.postpro == PP_ENFORCE_PERIOD) ? 1 : 0;
+            if (S0.fieldstart != 0 || S0.store_off != 0) return 0;
+            if (!fast_col_supported(L) || in_f64 != f64 || out_f64 != f64) return 0;
+            if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
+            if ((int64_t)(L + 1) * A.in_str[A.axis] >= (int64_t)INT32_MAX || (int64_t)(L + 1) * A.out_str[A.axis] >= (int64_t)INT32_MAX)
+                return 0;
+            if (k0 == LK_R2C) {
+                if (S0.in_cplx || !S0.out_cplx || A.n_src > L + extra || S0.n_store != L / 2 + 1 + extra) return 0;
+                if (extra && sp0.nfftw != L / 2 + 1) return 0;
+            } else {
+                if (!S0.in_cplx || S0.out_cplx || A.n_src != L / 2 + 1 + extra || S0.n_store > L + extra) return 0;
+                if (extra && (sp0.nfftw != L || S0.n_store != L + 1)) return 0;
+            }
+            return 3;
+        }
+        // r2r rows (DCT / DST I-IV): the post-processing is done by the kernel
+        if (k0 >= LK_DCT1 && k0 <= LK_DST4) {
+            if (A.fused || A.axis != 0 || !fast_r2r_supported(S0.M)) return 0;
+            for (int c = 0; c < A.lda; ++c) {
+                const LineSpec& sp = S0.spec[c];
+                if (sp.kind != k0 || sp.n_in != S0.spec[0].n_in || sp.fi != 0 || sp.fo != 0 ||
+                    sp.postpro != S0.spec[0].postpro || sp.nfftw != S0.spec[0].nfftw)
+                    return 0;
+            }
+            if (S0.fieldstart != 0 || S0.store_off != 0 || S0.in_cplx || S0.out_cplx) return 0;
+            if (A.n_src > S0.M || S0.n_store > S0.M || A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
+            if (f64 && (!in_f64 || !out_f64)) return 0;
+            return 4;
+        }
+    }
     const int nst = A.fused ? 2 : 1;
     for (int s2 = 0; s2 < nst; ++s2) {
         const LineStage& S = A.st[s2];
@@ -475,13 +520,14 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
     memset(&c, 0, sizeof(c));
     memset(&r, 0, sizeof(r));
     mode = 0;
-    if (kind == 1) {
+    if (kind == 1 || kind == 3) {
         c.in = A.in;
         c.out = A.out;
         c.nx = A.n_a;
         c.nouter = A.n_b;
         c.nin = A.n_src;
         c.nout = A.st[A.fused ? 1 : 0].n_store;
+        c.period = (kind == 3 && A.st[0].spec[0].postpro == PP_ENFORCE_PERIOD) ? A.st[0].spec[0].nfftw : -1;
         c.in_lstr = A.in_str[A.axis];
         c.in_ostr = A.in_str[b];
         c.in_cstr = A.in_cstr;
@@ -508,6 +554,11 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
     r.nrows = A.n_a * A.n_b;
     r.nin = A.n_src;
     r.nout = S0.n_store;
+    r.kind = S0.spec[0].kind;
+    r.n = S0.spec[0].n_in;
+    r.nstore = S0.n_store;
+    r.postpro = S0.spec[0].postpro;
+    r.nfftw = S0.spec[0].nfftw;
     r.in_s1 = A.in_str[1];
     r.in_s2 = A.in_str[2];
     r.in_cstr = A.in_cstr;
@@ -524,6 +575,17 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     RowArgs r;
     int mode = 0;
     fast_args(A, kind, in_f64, out_f64, c, r, mode);
+    if (kind == 4) {
+        r.tw2 = twiddle(L, f64);
+        r.tws = stage_table(L, f64);
+        check_cuda(launch_fast_r2r(f64, L, r, A.ncomp, stream), "r2r row launch");
+        return;
+    }
+    if (kind == 3) {
+        c.tws = stage_table(L, f64);
+        check_cuda(launch_fast_colreal(f64, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, stream), "column r2c/c2r launch");
+        return;
+    }
     if (kind == 1) {
         c.tws = stage_table(L, f64);
         if (force_tile) {

@@ -55,6 +55,15 @@ CASES = [
     ("unb48_hej2_r3", [48] * 3, 1, UNB3, CELL_CENTER, HEJ_2),
     ("unb96_48_192_r3", [96, 48, 192], 1, UNB3, CELL_CENTER, LGF_2),
     ("ppu96_hej4_r3", [96, 96, 48], 1, PPU, CELL_CENTER, HEJ_4),
+    # EVEN x (DCT line pass), UNB y and z: y is an r2c / c2r column pass
+    ("euu64_col_r2c", [64] * 3, 1, [[[0], [0]], [[4], [4]], [[4], [4]]], CELL_CENTER, HEJ_2),
+    ("euu48_col_r2c_r3", [48, 48, 96], 1, [[[0], [0]], [[4], [4]], [[4], [4]]], CELL_CENTER, LGF_2),
+    ("ppu48_rows48", [48] * 3, 1, PPU, CELL_CENTER, CHAT_2),
+    # node-centred EVEN/ODD x (DCT-III / DCT-II rows), PER y (r2c / c2r columns with the periodic copy), UNB z
+    ("node_eo_per_unb65", [65] * 3, 1, [[[0], [1]], [[3], [3]], [[4], [4]]], NODE_CENTER, HEJ_4),
+    ("node_eo_per_unb_129x65", [129, 65, 65], 1, [[[0], [1]], [[3], [3]], [[4], [4]]], NODE_CENTER, HEJ_4),
+    # cell-centred ODD/ODD x (DST rows), PER y and z
+    ("oopp64", [64] * 3, 1, [[[1], [1]], [[3], [3]], [[3], [3]]], CELL_CENTER, CHAT_2),
 ]
 
 
