@@ -469,7 +469,8 @@ def run_serve(args):
     FP32 (0.8) or FP64 (0.2); right-hand sides are seeded Gaussian sums resident on
     the device.  Runs the continuous-batching server from a cold cache, again with
     every key's solver resident, and a serial server (one solve at a time, no
-    batching) on the same warm cache.  One step = the whole trace."""
+    batching) on the same warm cache; then the same requests as one burst (all
+    arriving at t = 0) for the capacity of each.  One step = the whole trace."""
     import torch
     from flups_b200.serving import GpuBackend, Request, Server, latency_stats, make_trace, rhs_pool, run_trace
     torch.cuda.set_device(0)
@@ -493,20 +494,31 @@ def run_serve(args):
 
     def run(srv):
         srv.completed = []
+        s0, e0 = srv.setups, srv.evictions
         wall = run_trace(srv, trace, make)
         torch.cuda.synchronize()
         st = latency_stats(srv.completed)
         pts = sum(r.key[0] ** 3 for r in srv.completed)
         return {"wall_s": wall, "solves_per_s": len(srv.completed) / wall, "pts_per_s": pts / wall,
-                "mean_batch": float(np.mean([r.batch for r in srv.completed])), **st}
+                "mean_batch": float(np.mean([r.batch for r in srv.completed])),
+                "setups": srv.setups - s0, "evictions": srv.evictions - e0, **st}
 
     srv = Server(be, budget, max_batch=16)
     cold = run(srv)
-    cold.update({"setups": srv.setups, "evictions": srv.evictions})
     warm = run(srv)
     serial = Server(be, budget, max_batch=1, max_inflight=1)
     serial.cache, serial.reserved = srv.cache, srv.reserved
     ser = run(serial)
+    # capacity: the same requests arriving all at once (a burst), continuous vs
+    # serial; the first continuous burst grows every key's batch arrays (one
+    # allocation per key), the second runs on them
+    burst_trace = [(0.0, key, idx) for _, key, idx in trace]
+    saved = trace[:]
+    trace[:] = burst_trace
+    cap_first = run(srv)
+    cap = run(srv)
+    cap_serial = run(serial)
+    trace[:] = saved
     srv.close()
     line = {
         "metric": METRIC, "value": warm["pts_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
@@ -516,7 +528,8 @@ def run_serve(args):
                                "all-UNB/(PER,PER,UNB)/(EVEN,UNB,UNB), HEJ_2/LGF_2, fp32/fp64 0.8/0.2",
                    "budget_bytes": budget, "max_batch": 16},
         "p50_ms": warm["p50_ms"], "p99_ms": warm["p99_ms"],
-        "serve": {"continuous_warm": warm, "continuous_cold": cold, "serial_warm": ser},
+        "serve": {"continuous_warm": warm, "continuous_cold": cold, "serial_warm": ser,
+                  "burst_continuous_first": cap_first, "burst_continuous": cap, "burst_serial": cap_serial},
     }
     print(json.dumps(line), flush=True)
 

@@ -1,0 +1,12 @@
+// Half-length DCT / DST-III row kernels (row_dct_kernel, FAM 3):
+// FP64, and FP32 with the user's doubles on the input side, the output side
+// or neither.
+#include "fast_dft_impl.cuh"
+
+namespace flb {
+
+cudaError_t launch_dct3_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s) {
+    return launch_dct_types<3>(f64, in64, out64, n, a, ncomp, s);
+}
+
+}  // namespace flb

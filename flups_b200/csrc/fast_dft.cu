@@ -43,7 +43,26 @@ bool fast_r2r_supported(int M) {
     return false;
 }
 
+int fast_dct_family(int kind, int n, int M) {
+    if (M != 2 * n) return 0;
+    switch (n) {
+        case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: break;
+        default: return 0;
+    }
+    switch (kind) {
+        case LK_DCT2: case LK_DST2: return 2;
+        case LK_DCT3: case LK_DST3: return 3;
+        case LK_DCT4: case LK_DST4: return 4;
+    }
+    return 0;
+}
+
 cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s) {
+    switch (fast_dct_family(a.kind, a.n, M)) {
+        case 2: return launch_dct2_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);
+        case 3: return launch_dct3_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);
+        case 4: return launch_dct4_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);
+    }
     return launch_r2r_units(f64, a.in_f64, a.out_f64, M, a, ncomp, s);
 }
 

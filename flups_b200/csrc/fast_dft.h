@@ -83,6 +83,12 @@ cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncom
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 // r2r rows (DCT / DST I-IV) through an M-point complex register DFT
 bool fast_r2r_supported(int M);
+// DCT / DST II-IV rows of even length n (M = 2n) that run through one
+// n/2-point register DFT instead: the family (2, 3 or 4), else 0.  Their
+// tables: tw = W_n^q (q < n), tws = the stage table of the n/2-point DFT,
+// tw2 = W_2M^q as for the M-point kernel.
+int fast_dct_family(int kind, int n, int M);
+// launches the half-length kernel when fast_dct_family(a.kind, a.n, M) != 0
 cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
 // column r2c (c2r = 0: real in, X[0..L/2] out) and c2r (c2r = 1)
 cudaError_t launch_fast_colreal(int f64, int c2r, int L, const ColArgs& a, int ncomp, cudaStream_t s);

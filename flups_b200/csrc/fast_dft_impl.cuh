@@ -635,6 +635,161 @@ __global__ void __launch_bounds__(TR * (M / R1), (Occ<TR * (M / R1)>::blocks)) r
     }
 }
 
+// ---------------------------------------------------------------- rows: r2r, half length
+// DCT / DST II-IV of an even length n through one n/2-point complex register
+// DFT (LH = n/2) instead of the n- or 2n-point DFT of the extended row:
+//   II  (FAM 2): Makhoul's reordering v = (x_0, x_2, ..., x_3, x_1), the real
+//                n-point DFT V of v by the packed LH-point DFT and the split,
+//                Y_k = 2 Re(W_4n^k V_k), Y_{n-k} = -2 Im(W_4n^k V_k);
+//   III (FAM 3): the inverse: V_k = W_4n^{-k} (x_k - i x_{n-k}) (Hermitian),
+//                v = the real inverse DFT of V by the c2r pre-process and an
+//                LH-point inverse DFT, y_{2m} = v_m, y_{2m+1} = v_{n-1-m};
+//   IV  (FAM 4): t_j = (x_{2j} + i x_{n-1-2j}) W_8n^{4j+1}, T = DFT_LH(t),
+//                Y_{2k} = 2 Re(T_k W_4n^{2k}), Y_{n-1-2k} = -2 Im(T_k W_4n^{2k}).
+// The DST kinds reduce to the DCT ones: DST-II(x)_k = DCT-II((-1)^j x_j)_{n-1-k},
+// DST-III(x)_k = (-1)^k DCT-III(x_{n-1-j})_k, DST-IV(x)_k = (-1)^k DCT-IV(x_{n-1-j})_k.
+// The row is read with unit-stride loads (any alignment) and scattered to its
+// packed place in shared memory; the outputs are gathered back in row order, so
+// loads and stores are coalesced.  Outputs past n pass the input through and
+// the post-processing of the row (null first / last, period copy) is applied
+// as in row_r2r_kernel.  tw: W_n^q (q < n); tw2: W_4n^q; tws: the LH-point table.
+template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
+__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks)) row_dct_kernel(const RowArgs a) {
+    using F = RegFFT<T, LH, R1, true>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P, N = 2 * LH;
+    constexpr bool WSM = FAM != 4 && RowTw<T, LH>::SM;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int p = threadIdx.x % P, rr = threadIdx.x / P;
+    const int row = blockIdx.x * TR + rr;
+    const int comp = blockIdx.y;
+    const bool valid = row < a.nrows;
+    const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
+    const IT* src = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
+    C* line = sm + rr * F::SC;
+    T* lr = reinterpret_cast<T*>(line);
+    const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
+    C* wsm = sm + TR * F::SC + F::TW_SMEM;
+    if constexpr (WSM) {
+        stage_table_part<C, LH>(a.tw, wsm);
+        cp_async_commit();
+    }
+    const C* w4 = reinterpret_cast<const C*>(a.tw2);
+    const bool dst = (a.kind == LK_DST2 || a.kind == LK_DST3 || a.kind == LK_DST4);
+    const int nld = valid ? (a.nin < N ? a.nin : N) : 0;
+    const T z = (T)0;
+    // real m of the packed line: z_j = (r_{2j}, r_{2j+1}) at line[sw(j)]
+    auto slot = [](int m) { return 2 * F::sw(m >> 1) + (m & 1); };
+#pragma unroll
+    for (int r = 0; r < 2 * R1; ++r) {
+        const int i = p + P * r;
+        const T u = (i < nld) ? (T)src[i] : z;
+        int m;
+        if constexpr (FAM == 2) {
+            m = (i & 1) ? N - 1 - (i >> 1) : (i >> 1);
+        } else if constexpr (FAM == 3) {
+            m = i;
+        } else {
+            const int ii = dst ? N - 1 - i : i;
+            m = (ii & 1) ? N - ii : ii;  // x_{2j} -> r_{2j}; x_{n-1-2j} -> r_{2j+1}
+        }
+        lr[slot(m)] = (FAM == 2 && dst && (i & 1)) ? -u : u;
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    const C* wn = WSM ? wsm : reinterpret_cast<const C*>(a.tw);
+    C v[R1];
+    if constexpr (FAM == 2) {
+#pragma unroll
+        for (int r = 0; r < R1; ++r) v[r] = line[F::sw(p + P * r)];
+    } else if constexpr (FAM == 4) {
+        double ps, pc;
+        sincospi(-0.25 / (double)N, &ps, &pc);
+        const C w8 = mkc((T)pc, (T)ps);
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int j = p + P * r;
+            v[r] = cmul(cmul(line[F::sw(j)], w4[2 * j]), w8);
+        }
+    } else {
+        auto x = [&](int i) { return (i >= 0 && i < N) ? lr[slot(i)] : z; };
+        auto V = [&](int q) {
+            const T xa = dst ? x(N - 1 - q) : x(q), xb = dst ? x(q - 1) : x(N - q);
+            return cmulc(mkc(xa, -xb), w4[q]);  // W_4n^{-q} (xa - i xb)
+        };
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            C xk = V(k), xm = V(LH - k);
+            if (k == 0) {
+                xk.y = z;
+                xm.y = z;
+            }
+            xm = cconj(xm);
+            const C A = cadd(xk, xm);
+            const C B = cmul(csub(xk, xm), cconj(wn[k]));
+            v[r] = mkc(A.x - B.y, A.y + B.x);
+        }
+    }
+    F::template fft<false, FAM == 3>(v, line, p, tws);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    if constexpr (FAM == 2) {
+        // (Y_k, Y_{n-k}) at line[sw(k)], k < LH; (Y_0, Y_LH) at k = 0
+        __syncthreads();
+        constexpr T RT2 = (T)1.4142135623730950488;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            const C zk = v[r];
+            const C zm = cconj(line[F::sw(k == 0 ? 0 : LH - k)]);
+            const C e = cadd(zk, zm);
+            const C w = cmul(wn[k], csub(zk, zm));
+            const C Pk = cmul(w4[k], mkc((T)0.5 * (e.x + w.y), (T)0.5 * (e.y - w.x)));
+            v[r] = mkc((T)2 * Pk.x, (T)-2 * Pk.y);
+            if (r == 0 && p == 0) v[0].y = RT2 * (zk.x - zk.y);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    } else if constexpr (FAM == 4) {
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            const C u = cmul(v[r], w4[2 * k]);
+            line[F::sw(k)] = mkc((T)2 * u.x, (T)-2 * u.y);  // (Y_{2k}, Y_{n-1-2k})
+        }
+    }
+    __syncthreads();
+    if (!valid) return;
+    OT* out = reinterpret_cast<OT*>(a.out) + comp * a.out_cstr + (int64_t)i1 * a.out_s1 + (int64_t)i2 * a.out_s2;
+    auto value = [&](int i) -> T {
+        if constexpr (FAM == 2) {
+            const int k = dst ? N - 1 - i : i;
+            return k < LH ? line[F::sw(k)].x : (k == LH ? line[0].y : line[F::sw(N - k)].y);
+        } else if constexpr (FAM == 3) {
+            const T y = lr[slot((i & 1) ? N - 1 - (i >> 1) : (i >> 1))];
+            return (dst && (i & 1)) ? -y : y;
+        } else {
+            const T y = (i & 1) ? line[F::sw((N - 1 - i) >> 1)].y : line[F::sw(i >> 1)].x;
+            return (dst && (i & 1)) ? -y : y;
+        }
+    };
+    const bool first = a.postpro & PP_NULL_FIRST, last = a.postpro & PP_NULL_LAST, period = a.postpro & PP_ENFORCE_PERIOD;
+    for (int i = p; i < a.nstore; i += P) {
+        T y;
+        if (first && i == 0) y = z;
+        else if (last && i == a.nstore - 1) y = z;
+        else if (period && !first && !last && i == a.nfftw) y = value(0);
+        else if (i >= N) y = (i < a.nin) ? (T)src[i] : z;
+        else y = value(i);
+        out[i] = (OT)y;
+    }
+}
+
 // ---------------------------------------------------------------- rows: c2r
 // OT: type of the real output; HALF: nout = Lh (the row is truncated to half)
 template <typename T, typename OT, int LH, int R1, int TR, bool HALF>
@@ -715,6 +870,9 @@ cudaError_t launch_col_f64_m2(int sh, int L, const ColArgs& a, int ncomp, cudaSt
 cudaError_t launch_row_units(int f64, int c2r, int xt64, bool half, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_r2r_units(int f64, int in64, int out64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_dct2_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_dct3_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_dct4_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_colreal_f64(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 
 template <typename T, int L, int R1, int TX, int MODE, int SH>
@@ -854,6 +1012,51 @@ inline cudaError_t launch_r2r_len(int M, const RowArgs& a, int ncomp, cudaStream
         case 1024: return launch_r2r_t<T, IT, OT, 1024>(a, ncomp, s);
         case 2048: return launch_r2r_t<T, IT, OT, 2048>(a, ncomp, s);
     }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T, typename IT, typename OT, int LH, int FAM>
+inline cudaError_t launch_dct_t(const RowArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int R1 = fast_radix1_of(LH, sizeof(T) == 8);
+    using F = RegFFT<T, LH, R1, true>;
+    constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
+    const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0)) * sizeof(typename CT<T>::C);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(row_dct_kernel<T, IT, OT, LH, R1, TR, FAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((a.nrows + TR - 1) / TR, ncomp);
+    row_dct_kernel<T, IT, OT, LH, R1, TR, FAM><<<grid, TR * F::P, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// n: the (even) transform length; LH = n / 2
+template <typename T, typename IT, typename OT, int FAM>
+inline cudaError_t launch_dct_len(int n, const RowArgs& a, int ncomp, cudaStream_t s) {
+    switch (n) {
+        case 64: return launch_dct_t<T, IT, OT, 32, FAM>(a, ncomp, s);
+        case 96: return launch_dct_t<T, IT, OT, 48, FAM>(a, ncomp, s);
+        case 128: return launch_dct_t<T, IT, OT, 64, FAM>(a, ncomp, s);
+        case 192: return launch_dct_t<T, IT, OT, 96, FAM>(a, ncomp, s);
+        case 256: return launch_dct_t<T, IT, OT, 128, FAM>(a, ncomp, s);
+        case 384: return launch_dct_t<T, IT, OT, 192, FAM>(a, ncomp, s);
+        case 512: return launch_dct_t<T, IT, OT, 256, FAM>(a, ncomp, s);
+        case 768: return launch_dct_t<T, IT, OT, 384, FAM>(a, ncomp, s);
+        case 1024: return launch_dct_t<T, IT, OT, 512, FAM>(a, ncomp, s);
+        case 1536: return launch_dct_t<T, IT, OT, 768, FAM>(a, ncomp, s);
+        case 2048: return launch_dct_t<T, IT, OT, 1024, FAM>(a, ncomp, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int FAM>
+inline cudaError_t launch_dct_types(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s) {
+    if (f64) return launch_dct_len<double, double, double, FAM>(n, a, ncomp, s);
+    if (in64 && !out64) return launch_dct_len<float, double, float, FAM>(n, a, ncomp, s);
+    if (!in64 && out64) return launch_dct_len<float, float, double, FAM>(n, a, ncomp, s);
+    if (!in64 && !out64) return launch_dct_len<float, float, float, FAM>(n, a, ncomp, s);
     return cudaErrorInvalidValue;
 }
 

@@ -156,8 +156,14 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
         } else if (kinds[i] == 1 || kinds[i] == 3) {
             slot_for(A.st[0].M, 1);
         } else if (kinds[i] == 4) {
+            const LineSpec& sp = A.st[0].spec[0];
             slot_for(2 * A.st[0].M, 0);
-            slot_for(A.st[0].M, 1);
+            if (fast_dct_family(sp.kind, sp.n_in, A.st[0].M)) {
+                slot_for(sp.n_in, 0);
+                slot_for(sp.n_in / 2, 1);
+            } else {
+                slot_for(A.st[0].M, 1);
+            }
         } else {
             slot_for(A.st[0].M, 0);
             slot_for(A.st[0].M / 2, 1);
@@ -197,7 +203,12 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                 e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
             } else if (kinds[i] == 4) {
                 r.tw2 = tw_of(2 * L, 0);
-                r.tws = tw_of(L, 1);
+                if (fast_dct_family(r.kind, r.n, L)) {
+                    r.tw = tw_of(r.n, 0);
+                    r.tws = tw_of(r.n / 2, 1);
+                } else {
+                    r.tws = tw_of(L, 1);
+                }
                 e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
             } else {
                 r.tw = tw_of(L, 0);

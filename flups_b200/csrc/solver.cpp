@@ -455,7 +455,8 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
         }
         // r2r rows (DCT / DST I-IV): the post-processing is done by the kernel
         if (k0 >= LK_DCT1 && k0 <= LK_DST4) {
-            if (A.fused || A.axis != 0 || !fast_r2r_supported(S0.M)) return 0;
+            if (A.fused || A.axis != 0) return 0;
+            if (!fast_r2r_supported(S0.M) && !fast_dct_family(k0, S0.spec[0].n_in, S0.M)) return 0;
             for (int c = 0; c < A.lda; ++c) {
                 const LineSpec& sp = S0.spec[c];
                 if (sp.kind != k0 || sp.n_in != S0.spec[0].n_in || sp.fi != 0 || sp.fo != 0 ||
@@ -577,7 +578,12 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     fast_args(A, kind, in_f64, out_f64, c, r, mode);
     if (kind == 4) {
         r.tw2 = twiddle(L, f64);
-        r.tws = stage_table(L, f64);
+        if (fast_dct_family(r.kind, r.n, L)) {
+            r.tw = twiddle_plain(r.n, f64);
+            r.tws = stage_table(r.n / 2, f64);
+        } else {
+            r.tws = stage_table(L, f64);
+        }
         check_cuda(launch_fast_r2r(f64, L, r, A.ncomp, stream), "r2r row launch");
         return;
     }

@@ -7,8 +7,10 @@ set-up solvers -- plans and the Green's spectrum resident in HBM -- in a cache
 keyed by (grid, BCs, kernel, precision), so only the first request of a key
 pays the set-up.  It admits work by HBM footprint: a key's solver, its work
 arrays for the batch and the batch's staging arrays must fit in the memory
-budget; idle solvers are evicted least-recently-used when a new key needs
-room.  Continuous batching: every key has at most one batch in flight on its
+budget.  A batch shrinks (halving) until it fits in what is free; only when
+not even a single solve fits are idle solvers evicted, least-recently-used
+first, so a burst does not trade resident solvers (and their set-up time)
+for larger batches.  Continuous batching: every key has at most one batch in flight on its
 own CUDA stream; requests that arrive meanwhile queue and go out together
 (one flups_solve_batch launch per pass) as soon as the key's previous batch
 completes, while other keys' batches run concurrently on their streams.
@@ -74,21 +76,28 @@ class Server:
         return self.used() + need <= self.budget
 
     def _admit(self, key, nbatch):
-        """Handle for key sized for nbatch, or None when memory is short now."""
-        need = self.b.footprint(key, nbatch)
+        """(handle, nb) for key with the largest batch nb <= nbatch that fits
+        without evicting another key, or after evicting idle keys for a single
+        solve when nothing fits; (None, 0) while memory is short."""
         have = self.reserved.get(key, 0)
-        if key in self.cache and need <= have:
-            self.cache.move_to_end(key)
-            return self.cache[key]
-        extra = need - have
-        if not self._evict_for(extra):
-            return None
+        free = self.budget - self.used()
+        nb = nbatch
+        while nb >= 1:
+            need = self.b.footprint(key, nb)
+            if need - have <= free:
+                break
+            nb = nb // 2 if nb > 1 else 0
+        if nb == 0:
+            nb = 1
+            need = self.b.footprint(key, 1)
+            if not self._evict_for(need - have):
+                return None, 0
         if key not in self.cache:
             self.cache[key] = self.b.make(key)
             self.setups += 1
         self.cache.move_to_end(key)
-        self.reserved[key] = need
-        return self.cache[key]
+        self.reserved[key] = max(have, need)
+        return self.cache[key], nb
 
     # ---------------------------------------------------------------- loop
     def submit(self, req):
@@ -114,14 +123,9 @@ class Server:
             if self.max_inflight is not None and len(self.inflight) >= self.max_inflight:
                 break
             q = self.queues[key]
-            nb = min(len(q), self.max_batch)
-            h = self._admit(key, nb)
+            h, nb = self._admit(key, min(len(q), self.max_batch))
             if h is None:
-                if nb > 1:
-                    h = self._admit(key, 1)
-                    nb = 1
-                if h is None:
-                    continue
+                continue
             reqs = [q.popleft() for _ in range(nb)]
             for r in reqs:
                 r.batch = nb

@@ -64,6 +64,15 @@ CASES = [
     ("node_eo_per_unb_129x65", [129, 65, 65], 1, [[[0], [1]], [[3], [3]], [[4], [4]]], NODE_CENTER, HEJ_4),
     # cell-centred ODD/ODD x (DST rows), PER y and z
     ("oopp64", [64] * 3, 1, [[[1], [1]], [[3], [3]], [[3], [3]]], CELL_CENTER, CHAT_2),
+    # half-length DCT / DST rows: II/III (EVEN/EVEN, node ODD/EVEN), IV (EVEN/ODD, ODD/EVEN cell)
+    ("eepp128_dct23", [128, 32, 32], 1, [[[0], [0]], [[3], [3]], [[3], [3]]], CELL_CENTER, HEJ_2),
+    ("eopu64_dct4", [64] * 3, 1, [[[0], [1]], [[3], [3]], [[4], [4]]], CELL_CENTER, HEJ_4),
+    ("oeuu96_dst4_r3", [96, 48, 48], 1, [[[1], [0]], [[4], [4]], [[4], [4]]], CELL_CENTER, LGF_2),
+    ("node_oe_per_unb65_dst23", [65, 33, 33], 1, [[[1], [0]], [[3], [3]], [[4], [4]]], NODE_CENTER, CHAT_2),
+    ("vector3_eopu64_dct4", [64, 32, 32], 3, [[[0, 0, 0], [1, 1, 1]], [[3] * 3, [3] * 3], [[4] * 3, [4] * 3]],
+     CELL_CENTER, HEJ_2),
+    # node EVEN/EVEN x: DCT-I rows through the extended-row DFT
+    ("node_ee_unb65_dct1", [65, 33, 33], 1, [[[0], [0]], [[4], [4]], [[4], [4]]], NODE_CENTER, CHAT_2),
 ]
 
 

@@ -106,3 +106,29 @@ def test_serial_mode_one_at_a_time():
         assert len(srv.inflight) <= 1
     assert all(nb == 1 for _, nb in be.launches)
     assert len(srv.completed) == 5
+
+
+def test_batch_shrinks_before_evicting():
+    """Under a burst a resident key's batch is cut to what fits in the free
+    budget instead of evicting another resident solver."""
+    clk = Clock()
+    be = FakeBackend(per_key_bytes=100, per_rhs_bytes=10, steps=0)
+    srv = Server(be, budget_bytes=260, max_batch=8, clock=clk)
+    srv.submit(_req(0, "A", 0.0))
+    srv.submit(_req(1, "B", 0.0))
+    clk.t = 1
+    srv.poll()   # A and B resident at one rhs each: 220 bytes
+    for _ in range(3):
+        clk.t += 1
+        srv.poll()
+    assert srv.idle() and srv.used() == 220
+    for i in range(8):
+        srv.submit(_req(2 + i, "A", clk.t))
+    while not srv.idle():
+        clk.t += 1
+        srv.poll()
+    # 40 bytes free: A grows to 4 rhs at most (150 of 260 with B's 110)
+    sizes = [nb for k, nb in be.launches if k == "A"][1:]
+    assert sizes == [4, 4]
+    assert be.freed == [] and srv.evictions == 0 and srv.setups == 2
+    assert srv.used() <= 260
