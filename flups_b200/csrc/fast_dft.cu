@@ -1,6 +1,8 @@
 // Dispatch of the register-resident DFT passes (kernels in fast_dft_impl.cuh,
 // instantiated per precision and mode in fast_col_*.cu and fast_row.cu so
 // that the units compile in parallel).
+#include <cudaTypedefs.h>
+
 #include "fast_dft_impl.cuh"
 
 namespace flb {
@@ -22,6 +24,48 @@ bool fast_row_supported(int L) {
 }
 
 int fast_radix1(int f64, int n) { return fast_radix1_of(n, f64); }
+
+int fast_col_tile_width(int f64, int L, int tile) { return col_tile_threads(L, tile) / (L / fast_radix1_of(L, f64)); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    return fn;
+}
+
+bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const uint64_t strides[3], const uint32_t box[4],
+                   int nbox, int step, int dist) {
+    pf.nbox = 0;
+    auto fn = tensor_map_encoder();
+    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    cuuint64_t d[4], st[3];
+    cuuint32_t b[4], es[4] = {1, 1, 1, 1};
+    for (int i = 0; i < 4; ++i) {
+        if (dims[i] < 1 || dims[i] > (1ull << 32) || box[i] < 1 || box[i] > 256) return false;
+        d[i] = dims[i];
+        b[i] = box[i];
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (strides[i] % 16 != 0 || strides[i] >= (1ull << 40)) return false;
+        st[i] = strides[i];
+    }
+    if ((b[0] * 8) % 16 != 0) return false;
+    if (fn(&pf.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), d, st, b, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    pf.nbox = nbox;
+    pf.step = step;
+    pf.dist = dist;
+    return true;
+}
 
 int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1_of(n, f64)); }
 

@@ -1,10 +1,21 @@
 // Arguments and launchers of the register-resident power-of-two DFT passes
 // (fast_dft.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace flb {
+
+// L2 prefetch of the block `dist` launches ahead: a tensor map over the
+// pass's input (8-byte units, dims x, line / row, outer, component) and the
+// number of boxes per block along dim 0 (rows) or dim 1 (columns); nbox = 0
+// disables it.  The map is a member of the kernel's __grid_constant__
+// argument, so the TMA unit reads it from parameter space.
+struct Prefetch {
+    CUtensorMap map;
+    int nbox, dist, step;
+};
 
 struct ColArgs {
     const void* in;
@@ -22,6 +33,7 @@ struct ColArgs {
     double normfact;
     int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
     int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
+    Prefetch pf;            // column passes 0 / 1 along a short-stride axis
 };
 
 enum { COL_TILE_DEFAULT = 0, COL_TILE_256 = 1, COL_TILE_128 = 2 };
@@ -44,9 +56,18 @@ struct RowArgs {
     int nstore;             // outputs written (before post-processing)
     int postpro, nfftw;     // PostPro bits and the index PP_ENFORCE_PERIOD copies from 0
     const void* tw2;        // W_{2M}^q, q < 2M (pre/post twiddles of the r2r kinds)
+    Prefetch pf;            // r2c / c2r rows
 };
 
+// Fills `pf` for a 4-D view of 8-byte units (dims[0] fastest; strides in
+// bytes of dims 1..3) with box `box`; false (pf.nbox = 0) when the view does
+// not meet the tensor-map rules (16-byte aligned base and strides).
+bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const uint64_t strides[3], const uint32_t box[4],
+                   int nbox, int step, int dist);
+
 bool fast_col_supported(int L);
+// columns per CTA of a column pass of length L with CTA tile `tile`
+int fast_col_tile_width(int f64, int L, int tile);
 bool fast_row_supported(int L);
 
 // First radix of the register DFTs for an n-point line: 32 in FP32 and 16 in

@@ -182,6 +182,35 @@ struct RegFFT {
     }
 };
 
+// TMA prefetch into L2 of one box of a 4-D tensor map (a hint: no
+// shared memory, no completion to wait for)
+__device__ __forceinline__ void l2_prefetch_box(const CUtensorMap* m, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(reinterpret_cast<uint64_t>(m)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
+// the input of the block `pf.dist` launches after this one (blocks launch
+// in x, y, z order): columns prefetch boxes along the line (dim 1), rows
+// along the row (dim 0)
+template <bool ROWS>
+__device__ __forceinline__ void prefetch_ahead(const Prefetch& pf, int units_per_block, int rows_n1) {
+    if (pf.nbox == 0 || threadIdx.x != 0) return;
+    const long long lin = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z) + pf.dist;
+    const int bx = (int)(lin % gridDim.x);
+    const long long rest = lin / gridDim.x;
+    const int by = (int)(rest % gridDim.y), bz = (int)(rest / gridDim.y);
+    if (bz >= (int)gridDim.z) return;
+    if constexpr (ROWS) {
+        // block bx holds rows bx * units_per_block ... ; dim 1 = i1, dim 2 = i2, dim 3 = component (grid y)
+        const int row0 = bx * units_per_block;
+        const int i1 = row0 % rows_n1, i2 = row0 / rows_n1;
+        for (int k = 0; k < pf.nbox; ++k) l2_prefetch_box(&pf.map, k * pf.step, i1, i2, by);
+    } else {
+        for (int k = 0; k < pf.nbox; ++k) l2_prefetch_box(&pf.map, bx * units_per_block, k * pf.step, by, bz);
+    }
+}
+
 __device__ __forceinline__ int fold_idx(int i, int M) { return (M > 0 && 2 * i > M) ? M - i : i; }
 
 // asynchronous global -> shared copies (LDGSTS): the stage twiddles and the
@@ -304,7 +333,7 @@ enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
 //      2: forward, Green multiply, inverse (SH: loaded and stored part).
 // The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
 template <typename T, int L, int R1, int TX, int MODE, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2>::blocks)) col_dft_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2>::blocks)) col_dft_kernel(const __grid_constant__ ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
@@ -318,6 +347,7 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2>:
     const int o = (MODE == 2) ? mirror_order(blockIdx.y, a.nouter, a.f_outer) : (int)blockIdx.y;
     const int comp = blockIdx.z;
     const bool valid = x < a.nx;
+    if constexpr (MODE != 2) prefetch_ahead<false>(a.pf, TX * (int)(sizeof(C) / 8), 0);
     // shared memory: TX lines of the exchange, the stage table, the Green's values
     const C* tws = stage_twiddles<F>(a.tws, sm + TX * F::SC);
     T* gs = reinterpret_cast<T*>(sm + TX * F::SC + F::TW_SMEM);
@@ -458,7 +488,7 @@ template <> struct Vec2<double> { using V = double2; };
 // IT: type of the real input (the user's double array, or the working precision);
 // HALF: nin = Lh (the row is zero-padded to twice its length)
 template <typename T, typename IT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_r2c_kernel(const RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_r2c_kernel(const __grid_constant__ RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     using V = typename Vec2<IT>::V;
@@ -469,6 +499,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     const int comp = blockIdx.y;
     const bool valid = row < a.nrows;
     const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
+    prefetch_ahead<true>(a.pf, TR, a.n1);
     // rows past the end read the array's first elements and drop them (no branch)
     const IT* src = valid ? reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2 + 2 * p
                           : reinterpret_cast<const IT*>(a.in);
@@ -793,7 +824,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
 // ---------------------------------------------------------------- rows: c2r
 // OT: type of the real output; HALF: nout = Lh (the row is truncated to half)
 template <typename T, typename OT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_c2r_kernel(const RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_c2r_kernel(const __grid_constant__ RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     using V = typename Vec2<OT>::V;
@@ -804,6 +835,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) r
     const int comp = blockIdx.y;
     const bool valid = row < a.nrows;
     const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
+    prefetch_ahead<true>(a.pf, TR, a.n1);
     C* line = sm + rr * F::SC;
     const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
     C* wsm = sm + TR * F::SC + F::TW_SMEM;

@@ -232,6 +232,10 @@ struct Solver {
     void bwd_pass(int ip, double* user_out, int type, int nbatch);
     // overlapped middle passes over x-slabs (flups_b200_set_overlap)
     bool overlap = false;
+    // L2 prefetch of the next blocks' input in the row and column passes (flups_b200_set_prefetch)
+    bool prefetch = true;
+    void col_prefetch(flb::ColArgs& c, bool f64, int L, int ncomp) const;
+    void row_prefetch(flb::RowArgs& r, bool f64, bool c2r, int L, int ncomp) const;
     static constexpr int kOvSlabs = 4;
     cudaStream_t ov_stream[2] = {nullptr, nullptr};
     cudaEvent_t ov_ev0 = nullptr, ov_evf[kOvSlabs] = {}, ov_evg[kOvSlabs] = {};

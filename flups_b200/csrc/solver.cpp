@@ -600,12 +600,47 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
             auto it = tuned_tile.find(pass_key(A, f64));
             if (it != tuned_tile.end()) c.tile = it->second;
         }
+        if (prefetch && mode != 2) col_prefetch(c, f64, L, A.ncomp);
         check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
         return;
     }
     r.tw = twiddle_plain(L, f64);
     r.tws = stage_table(L / 2, f64);
-    check_cuda(launch_fast_row(f64, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, stream), "row DFT launch");
+    const bool c2r = A.st[0].spec[0].kind == LK_C2R;
+    if (prefetch) row_prefetch(r, f64, c2r, L, A.ncomp);
+    check_cuda(launch_fast_row(f64, c2r, L, r, A.ncomp, stream), "row DFT launch");
+}
+
+// L2 prefetch of the next blocks' input for the forward / inverse column
+// passes along a short-stride axis (lines farther apart than 64 KB touch a
+// DRAM page per element and gain nothing) and for the r2c / c2r rows.
+static constexpr int PREFETCH_DIST = 148;
+
+void Solver::col_prefetch(ColArgs& c, bool f64, int L, int ncomp) const {
+    const int es = f64 ? 16 : 8, u = es / 8;
+    if ((int64_t)c.in_lstr * es > 65536) return;
+    const int tx = fast_col_tile_width(f64 ? 1 : 0, L, c.tile);
+    const uint64_t outer_bytes = (uint64_t)c.in_ostr * es;
+    const uint64_t dims[4] = {(uint64_t)c.nx * u, (uint64_t)c.nin, (uint64_t)c.nouter, (uint64_t)ncomp};
+    const uint64_t strides[3] = {(uint64_t)c.in_lstr * es, outer_bytes,
+                                 ncomp > 1 ? (uint64_t)c.in_cstr * es : outer_bytes * (uint64_t)c.nouter};
+    const uint32_t box[4] = {(uint32_t)(tx * u), (uint32_t)std::min(256, c.nin), 1, 1};
+    make_prefetch(c.pf, c.in, dims, strides, box, (c.nin + 255) / 256, 256, PREFETCH_DIST);
+}
+
+void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) const {
+    const int lh = L / 2;
+    const int elem = c2r ? (f64 ? 16 : 8) : (r.in_f64 ? 8 : 4);
+    const uint64_t row_bytes = (uint64_t)r.nin * elem;
+    const uint64_t units = (row_bytes + 7) / 8;
+    const int p = lh / fast_radix1(f64 ? 1 : 0, lh);
+    const int tr = p >= 256 ? 1 : 256 / p;
+    const uint64_t n2 = (uint64_t)(r.nrows / r.n1);
+    const uint64_t s2 = (uint64_t)r.in_s2 * elem;
+    const uint64_t dims[4] = {units, (uint64_t)r.n1, n2, (uint64_t)ncomp};
+    const uint64_t strides[3] = {(uint64_t)r.in_s1 * elem, s2, ncomp > 1 ? (uint64_t)r.in_cstr * elem : s2 * n2};
+    const uint32_t box[4] = {(uint32_t)std::min<uint64_t>(256, (units + 1) / 2 * 2), (uint32_t)std::min(tr, r.n1), 1, 1};
+    make_prefetch(r.pf, r.in, dims, strides, box, (int)((units + 255) / 256), 256, PREFETCH_DIST);
 }
 
 const void* Solver::stage_table(int n, bool f64) {

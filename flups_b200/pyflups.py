@@ -115,6 +115,7 @@ def load_library(path=None):
         "flups_b200_set_autotune": (None, [vp, c_int]),
         "flups_b200_set_col_tile": (None, [vp, c_int]),
         "flups_b200_set_overlap": (None, [vp, c_int]),
+        "flups_b200_set_prefetch": (None, [vp, c_int]),
         "flups_get_innerBuffer": (vp, [vp]),
         "flups_get_innerTopo_physical": (vp, [vp]),
         "flups_get_innerTopo_spectral": (vp, [vp]),
@@ -307,6 +308,10 @@ class Solver:
     def set_overlap(self, on):
         """Overlap the per-x-slab middle passes on three streams (device arrays, STD)."""
         _lib.flups_b200_set_overlap(self._solver, int(bool(on)))
+
+    def set_prefetch(self, on):
+        """L2 prefetch of the next blocks' input in the row / column passes (default on)."""
+        _lib.flups_b200_set_prefetch(self._solver, int(bool(on)))
 
     def set_col_tile(self, tile):
         """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""

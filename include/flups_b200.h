@@ -88,6 +88,13 @@ void flups_b200_set_autotune(struct Solver* s, int on);
  * identical.  No reference counterpart. */
 void flups_b200_set_overlap(struct Solver* s, int on);
 
+/* L2 prefetch in the register-DFT row passes and the forward / inverse
+ * column passes (1 = on, the default): each CTA asks the TMA unit to bring
+ * the input of the CTA launched 148 blocks later into L2, so that CTA's
+ * loads hit L2.  Results are identical either way.  No reference
+ * counterpart. */
+void flups_b200_set_prefetch(struct Solver* s, int on);
+
 /* Force the CTA tile of every column pass: 0 = default or tuned, 1 = 256
  * threads, 2 = 128 threads.  For cross-checking the tiles. */
 void flups_b200_set_col_tile(struct Solver* s, int tile);
