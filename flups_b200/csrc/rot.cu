@@ -16,63 +16,70 @@
 
 namespace flb {
 
+// Block = 128 x-positions of one y row and a chunk of zb z values (of one
+// component for STD, of one 3-component group for ROT): no index division
+// per element, the x and y parts of the wave numbers and of the Green's
+// index are computed once per thread, the z part once per z.  Wave numbers
+// are evaluated in FP64 and rounded once to the data precision, in which the
+// per-element curl and scaling run.
 template <typename TD, typename TG>
-__global__ void __launch_bounds__(256) spec_mult_kernel(const RotArgs A) {
+__global__ void __launch_bounds__(128) spec_mult_kernel(const __grid_constant__ RotArgs A, int zb) {
     using C = typename CT<TD>::C;
+    using T = TD;
     const MultSpec& G = A.mult;
-    const int64_t n0 = A.n[0], n1 = A.n[1], n2 = A.n[2];
-    const int64_t per = n0 * n1 * n2;
-    const int64_t groups = (G.mode == 2) ? A.nbatch : A.ncomp;  // ROT: 3 components per group
-    const int64_t total = per * groups;
-    C* data = reinterpret_cast<C*>(A.data);
+    const int x = blockIdx.x * 128 + threadIdx.x;
+    if (x >= A.n[0]) return;
+    const int y = blockIdx.y;
+    const int nzc = (A.n[2] + zb - 1) / zb;
+    const int grp = blockIdx.z / nzc, z0 = (blockIdx.z % nzc) * zb;
+    const int z1 = min(z0 + zb, A.n[2]);
     const TG* green = reinterpret_cast<const TG*>(G.green);
-    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t b = id / per, r = id - b * per;
-        int idx[3];
-        idx[0] = (int)(r % n0);
-        idx[1] = (int)((r / n0) % n1);
-        idx[2] = (int)(r / (n0 * n1));
-        int64_t go = 0, off = 0;
-        for (int d = 0; d < 3; ++d) {
-            go += (int64_t)gfold(idx[d], G.gfold[d]) * G.gstr[d];
-            off += (int64_t)idx[d] * A.str[d];
+    const int64_t gxy = (int64_t)gfold(x, G.gfold[0]) * G.gstr[0] + (int64_t)gfold(y, G.gfold[1]) * G.gstr[1];
+    const int64_t oxy = (int64_t)x * A.str[0] + (int64_t)y * A.str[1];
+    C* data = reinterpret_cast<C*>(A.data);
+    if (G.mode != 2) {
+        C* p = data + grp * A.cstr + oxy;
+        for (int z = z0; z < z1; ++z) {
+            const double g = (double)green[gxy + (int64_t)gfold(z, G.gfold[2]) * G.gstr[2]] * G.normfact;
+            C* q = p + (int64_t)z * A.str[2];
+            *q = mkc((TD)(q->x * g), (TD)(q->y * g));
         }
-        const double g = (double)green[go] * G.normfact;
-        if (G.mode != 2) {
-            C* p = data + b * A.cstr + off;
-            *p = mkc((TD)(p->x * g), (TD)(p->y * g));
-            continue;
-        }
-        double kk[3];
-        for (int d = 0; d < 3; ++d) kk[d] = (double)symid(idx[d], G.symstart[d]) + G.koffset[d];
-        auto kc = [&](int d, int c) {
-            return make_double2(fd_symbol(G.odiff, kk[d] * G.kfact[d][c][0], G.hgrid[d]),
-                                fd_symbol(G.odiff, kk[d] * G.kfact[d][c][1], G.hgrid[d]));
-        };
-        C* p0 = data + (3 * b + 0) * A.cstr + off;
-        C* p1 = data + (3 * b + 1) * A.cstr + off;
-        C* p2 = data + (3 * b + 2) * A.cstr + off;
-        const double2 f0 = make_double2(p0->x, p0->y);
-        const double2 f1 = make_double2(p1->x, p1->y);
-        const double2 f2 = make_double2(p2->x, p2->y);
-        const double2 r0 = csub(cmul(f2, kc(1, 2)), cmul(f1, kc(2, 1)));
-        const double2 r1 = csub(cmul(f0, kc(2, 0)), cmul(f2, kc(0, 2)));
-        const double2 r2 = csub(cmul(f1, kc(0, 1)), cmul(f0, kc(1, 0)));
-        *p0 = mkc((TD)(r0.x * g), (TD)(r0.y * g));
-        *p1 = mkc((TD)(r1.x * g), (TD)(r1.y * g));
-        *p2 = mkc((TD)(r2.x * g), (TD)(r2.y * g));
+        return;
+    }
+    // K_d for component c: (symbol((is_d + koffset_d) kfact_dc0), symbol(... kfact_dc1))
+    auto kc = [&](int d, int i, int c) {
+        const double kk = (double)symid(i, G.symstart[d]) + G.koffset[d];
+        return mkc((T)fd_symbol(G.odiff, kk * G.kfact[d][c][0], G.hgrid[d]), (T)fd_symbol(G.odiff, kk * G.kfact[d][c][1], G.hgrid[d]));
+    };
+    const C kx1 = kc(0, x, 1), kx2 = kc(0, x, 2), ky0 = kc(1, y, 0), ky2 = kc(1, y, 2);
+    const T nf = (T)G.normfact;
+    C* p0 = data + (3 * grp + 0) * A.cstr + oxy;
+    C* p1 = data + (3 * grp + 1) * A.cstr + oxy;
+    C* p2 = data + (3 * grp + 2) * A.cstr + oxy;
+    for (int z = z0; z < z1; ++z) {
+        const int64_t o = (int64_t)z * A.str[2];
+        const C kz0 = kc(2, z, 0), kz1 = kc(2, z, 1);
+        const T g = (T)green[gxy + (int64_t)gfold(z, G.gfold[2]) * G.gstr[2]] * nf;
+        const C f0 = p0[o], f1 = p1[o], f2 = p2[o];
+        const C r0 = csub(cmul(f2, ky2), cmul(f1, kz1));
+        const C r1 = csub(cmul(f0, kz0), cmul(f2, kx2));
+        const C r2 = csub(cmul(f1, kx1), cmul(f0, ky0));
+        p0[o] = mkc(r0.x * g, r0.y * g);
+        p1[o] = mkc(r1.x * g, r1.y * g);
+        p2[o] = mkc(r2.x * g, r2.y * g);
     }
 }
 
 cudaError_t launch_spec_mult(const RotArgs& A, int data_f64, int green_f64, cudaStream_t s) {
-    const int64_t groups = (A.mult.mode == 2) ? A.nbatch : A.ncomp;
-    const int64_t total = (int64_t)A.n[0] * A.n[1] * A.n[2] * groups;
-    int64_t nb = (total + 255) / 256;
-    if (nb > 148 * 32) nb = 148 * 32;
-    if (nb < 1) return cudaSuccess;
-    if (data_f64 && green_f64) spec_mult_kernel<double, double><<<(unsigned)nb, 256, 0, s>>>(A);
-    else if (data_f64) spec_mult_kernel<double, float><<<(unsigned)nb, 256, 0, s>>>(A);
-    else spec_mult_kernel<float, float><<<(unsigned)nb, 256, 0, s>>>(A);
+    const int groups = (A.mult.mode == 2) ? A.nbatch : A.ncomp;
+    if ((int64_t)A.n[0] * A.n[1] * A.n[2] * groups == 0) return cudaSuccess;
+    const int zb = 32;
+    const int nzc = (A.n[2] + zb - 1) / zb;
+    if (A.n[1] > 65535 || (int64_t)nzc * groups > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((A.n[0] + 127) / 128, A.n[1], nzc * groups);
+    if (data_f64 && green_f64) spec_mult_kernel<double, double><<<grid, 128, 0, s>>>(A, zb);
+    else if (data_f64) spec_mult_kernel<double, float><<<grid, 128, 0, s>>>(A, zb);
+    else spec_mult_kernel<float, float><<<grid, 128, 0, s>>>(A, zb);
     return cudaGetLastError();
 }
 
