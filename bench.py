@@ -55,6 +55,9 @@ def parse():
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
     ap.add_argument("--overlap", type=int, default=0, help="1: overlap the per-x-slab middle passes on three streams")
+    ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="with --profile: an all-unbounded grid NX x NY x NZ instead of n^3 (for ncu captures of one pass "
+                         "length on a smaller array, e.g. 256 256 512 runs the 1024-point fused z pass on 1/4 of the lines)")
     return ap.parse_args()
 
 
@@ -534,6 +537,35 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_grid(args):
+    """FP32 solves of a seeded random right-hand side on an anisotropic all-unbounded
+    grid (cell-centred, h = 1/NX), for ncu captures; prints the mean solve time."""
+    import torch
+    from flups_b200 import pyflups as pf
+    nx, ny, nz = args.grid
+    torch.cuda.set_device(0)
+    B = pf.BoundaryType
+    t = pf.Topology(0, 1, [nx, ny, nz])
+    s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1.0 / nx] * 3, [1.0, ny / nx, nz / nx])
+    s.set_green_type(pf.GreenType[args.kernel])
+    s.set_precision(32)
+    s.setup()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    rhs = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=g)
+    field = torch.empty_like(rhs)
+    for _ in range(max(1, args.warmup)):
+        s.solve(field, rhs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        s.solve(field, rhs)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": True, "grid": [nx, ny, nz], "ms_per_step": e0.elapsed_time(e1) / args.steps}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -547,6 +579,9 @@ def main():
         return
     if args.workload in ("config2", "config3"):
         run_config(args)
+        return
+    if args.profile and args.grid:
+        run_profile_grid(args)
         return
     import torch
     import torch.distributed as dist

@@ -691,6 +691,15 @@ __global__ void __launch_bounds__(TR * (M / R1), (Occ<TR * (M / R1)>::blocks)) r
 // loads and stores are coalesced.  Outputs past n pass the input through and
 // the post-processing of the row (null first / last, period copy) is applied
 // as in row_r2r_kernel.  tw: W_n^q (q < n); tw2: W_4n^q; tws: the LH-point table.
+// W_4n^q entries a half-length DCT family uses (q <= LH; IV: q < n), staged in
+// shared memory when they take at most 8 KB
+template <typename T, int FAM, int LH>
+struct DctW4 {
+    static constexpr int USED = (FAM == 4) ? 2 * LH : LH + 1;
+    static constexpr bool SM = USED * (int)sizeof(typename CT<T>::C) <= 8192;
+    static constexpr int N = SM ? USED : 0;
+};
+
 template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
 __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks)) row_dct_kernel(const RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
@@ -709,11 +718,15 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
     T* lr = reinterpret_cast<T*>(line);
     const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
     C* wsm = sm + TR * F::SC + F::TW_SMEM;
-    if constexpr (WSM) {
-        stage_table_part<C, LH>(a.tw, wsm);
-        cp_async_commit();
-    }
+    if constexpr (WSM) stage_table_part<C, LH>(a.tw, wsm);
+    // the W_4n^q of this family, staged while the row loads are in flight
     const C* w4 = reinterpret_cast<const C*>(a.tw2);
+    if constexpr (DctW4<T, FAM, LH>::SM) {
+        C* w4s = wsm + (WSM ? LH : 0);
+        for (int e = threadIdx.x; e < DctW4<T, FAM, LH>::N; e += blockDim.x) cp_async<sizeof(C)>(w4s + e, w4 + e);
+        w4 = w4s;
+    }
+    cp_async_commit();
     const bool dst = (a.kind == LK_DST2 || a.kind == LK_DST3 || a.kind == LK_DST4);
     const int nld = valid ? (a.nin < N ? a.nin : N) : 0;
     const T z = (T)0;
@@ -1059,7 +1072,8 @@ inline cudaError_t launch_dct_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = fast_radix1_of(LH, sizeof(T) == 8);
     using F = RegFFT<T, LH, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
-    const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0)) * sizeof(typename CT<T>::C);
+    const size_t smem =
+        (size_t)(TR * F::SC + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0) + DctW4<T, FAM, LH>::N) * sizeof(typename CT<T>::C);
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(row_dct_kernel<T, IT, OT, LH, R1, TR, FAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
