@@ -142,11 +142,12 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per launch / algorithmic bytes per launch of each pass,
-# from one ncu capture of the same kernels on the 256^3 case
-# (profiles/col_dft_256cube_fp32_full.md, profiles/row_dft_256cube_fp32_full.md);
-# the traffic of a 512^3 launch is this ratio times its algorithmic bytes
-# (traffic grows with the lines processed)
-TRAFFIC_RATIO_256 = {"fused": 583.7 / 606.9, "fwd1": 369.0 / 404.2, "bwd1": 397.7 / 404.2,
+# from one ncu capture of the same kernel on a smaller array: the fused z pass
+# (1024-point lines) on the 256 x 256 x 512 grid (1219.8 MB of DRAM traffic for
+# 1213.5 MB algorithmic), the other passes on 256^3; the traffic of a 512^3
+# launch is this ratio times its algorithmic bytes (traffic grows with the
+# lines processed)
+TRAFFIC_RATIO_256 = {"fused": 1219.8 / 1213.5, "fwd1": 369.0 / 404.2, "bwd1": 397.7 / 404.2,
                      "fwd0": 228.8 / 269.1, "bwd0": 228.4 / 269.1}
 
 
@@ -681,6 +682,25 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_ms = float(tt.item())
     user_bytes = n ** 3 * 8
+    # the bound of that path: the same bytes copied up and down at once on two
+    # streams (pinned memory, PCIe both ways), no solve
+    d_up = torch.empty_like(rhs)
+    cs1, cs2 = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    for rep in range(2):
+        torch.cuda.synchronize()
+        c0.record(cs1)
+        cs2.wait_event(c0)
+        with torch.cuda.stream(cs1):
+            d_up.copy_(h_rhs, non_blocking=True)
+        with torch.cuda.stream(cs2):
+            h_out.copy_(field, non_blocking=True)
+        cs1.wait_stream(cs2)
+        c1.record(cs1)
+        c1.synchronize()
+    pcie_ms = c0.elapsed_time(c1)
+    del d_up
 
     # ---------------------------------------------------------------- FP64 mode and the FP32 error
     del s32, t32
@@ -731,13 +751,16 @@ def main():
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (TRAFFIC_RATIO_256[dom["name"]] * dom["bytes"]
                                  if (n == 512 and args.kernel == "LGF_2" and dom["name"] in TRAFFIC_RATIO_256) else None),
-                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum of the 256^3 launch, scaled by lines",
+                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum of the same kernel on a smaller grid "
+                                       "(fused: 256x256x512, others: 256^3), scaled by lines",
                      "bytes_per_launch": dom["bytes"], "ms_per_launch": dom_ms,
                      "solve_bytes": tot_bytes, "solve_frac": tot_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
                      "passes": [{"name": p["name"], "ms": p["ms_total"] / max(1, p["calls"]), "bytes": p["bytes"]} for p in stats]},
         "e2e": {"value": world * n ** 3 / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": user_bytes,
                 "d2h_bytes_per_step": user_bytes, "ms_per_step": e2e_ms, "steps": e2e_steps,
-                "path": "flups_solve with pinned host rhs/field, async: slab-streamed upload/download overlapped"},
+                "path": "flups_solve with pinned host rhs/field, async: slab-streamed upload/download overlapped",
+                "pcie_bound_ms": pcie_ms,
+                "pcie_bound_note": "the step's H2D and D2H bytes copied at once on two streams, no solve"},
         "gpu_launches": launches_per_solve * args.steps,
         "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.sample_n}^3 solves of the same workload, FP64 oracle (numpy/scipy restatement), median of 3"},
