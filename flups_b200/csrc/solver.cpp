@@ -615,10 +615,13 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
 // passes along a short-stride axis (lines farther apart than 64 KB touch a
 // DRAM page per element and gain nothing) and for the r2c / c2r rows.
 static constexpr int PREFETCH_DIST = 148;
+// inputs smaller than this stay in the 126 MB L2 anyway: no tensor map is built
+static constexpr double PREFETCH_MIN_BYTES = 64.0 * 1024 * 1024;
 
 void Solver::col_prefetch(ColArgs& c, bool f64, int L, int ncomp) const {
     const int es = f64 ? 16 : 8, u = es / 8;
     if ((int64_t)c.in_lstr * es > 65536) return;
+    if ((double)c.nx * c.nin * c.nouter * ncomp * es < PREFETCH_MIN_BYTES) return;
     const int tx = fast_col_tile_width(f64 ? 1 : 0, L, c.tile);
     const uint64_t outer_bytes = (uint64_t)c.in_ostr * es;
     const uint64_t dims[4] = {(uint64_t)c.nx * u, (uint64_t)c.nin, (uint64_t)c.nouter, (uint64_t)ncomp};
@@ -632,6 +635,7 @@ void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) cons
     const int lh = L / 2;
     const int elem = c2r ? (f64 ? 16 : 8) : (r.in_f64 ? 8 : 4);
     const uint64_t row_bytes = (uint64_t)r.nin * elem;
+    if ((double)row_bytes * r.nrows * ncomp < PREFETCH_MIN_BYTES) return;
     const uint64_t units = (row_bytes + 7) / 8;
     const int p = lh / fast_radix1(f64 ? 1 : 0, lh);
     const int tr = p >= 256 ? 1 : 256 / p;

@@ -1,5 +1,6 @@
 """Batched solves replayed from CUDA graphs, the CTA-tile autotuner and the
-two compiled column tiles: none of them changes the per-line arithmetic, so
+two compiled column tiles, the x-slab overlap and the L2 prefetch: none of
+them changes the per-line arithmetic, so
 each must reproduce the plain solve bit for bit (one right-hand side and a
 batch, FP32 and FP64, lines of 64 to 512 points)."""
 import numpy as np
@@ -86,4 +87,24 @@ def test_overlapped_middle_passes_bitwise(n, precision):
         s.solve(out, rhs)
         torch.cuda.synchronize()
         assert torch.equal(out, ref)
+    assert s.last_error() == 0
+
+
+@pytest.mark.parametrize("n,precision,nb", [(256, 32, 1), (256, 64, 1), (128, 32, 8)])
+def test_l2_prefetch_bitwise(n, precision, nb):
+    """The TMA L2 prefetch of the next blocks' input (row and column passes
+    whose input exceeds 64 MB) is a hint only: results with it on and off are
+    identical, for one right-hand side and for a batch."""
+    import torch
+    t, s = _setup(n, LGF_2, precision)
+    rhs = torch.from_numpy(_rhs(n, nb, 11)).cuda()
+    s.set_prefetch(False)
+    ref = torch.zeros_like(rhs)
+    s.solve_batch(ref, rhs, nb) if nb > 1 else s.solve(ref, rhs)
+    torch.cuda.synchronize()
+    s.set_prefetch(True)
+    out = torch.full_like(rhs, float("nan"))
+    s.solve_batch(out, rhs, nb) if nb > 1 else s.solve(out, rhs)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
     assert s.last_error() == 0
