@@ -27,6 +27,7 @@
 #include "cplx.cuh"
 #include "fast_dft.h"
 #include "pass_desc.h"
+#include "smem_attr.cuh"
 
 namespace flb {
 
@@ -932,13 +933,8 @@ inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, L, R1>;
     const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C) +
                         (MODE == 2 ? (size_t)GStage<L>::N * TX * sizeof(T) : 0);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(col_dft_kernel<T, L, R1, TX, MODE, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, col_dft_kernel<T, L, R1, TX, MODE, SH>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
     col_dft_kernel<T, L, R1, TX, MODE, SH><<<grid, TX * F::P, smem, s>>>(a);
     return cudaGetLastError();
@@ -989,12 +985,8 @@ inline cudaError_t launch_colreal_t(const ColArgs& a, int ncomp, cudaStream_t s)
     static_assert(TX >= 1, "tile narrower than one column");
     using F = RegFFT<T, L, R1>;
     const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(col_real_kernel<T, L, R1, TX, C2R, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, col_real_kernel<T, L, R1, TX, C2R, SH>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
     col_real_kernel<T, L, R1, TX, C2R, SH><<<grid, TX * F::P, smem, s>>>(a);
     return cudaGetLastError();
@@ -1039,12 +1031,8 @@ inline cudaError_t launch_r2r_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, M, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(row_r2r_kernel<T, IT, OT, M, R1, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, row_r2r_kernel<T, IT, OT, M, R1, TR>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nrows + TR - 1) / TR, ncomp);
     row_r2r_kernel<T, IT, OT, M, R1, TR><<<grid, TR * F::P, smem, s>>>(a);
     return cudaGetLastError();
@@ -1074,12 +1062,8 @@ inline cudaError_t launch_dct_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem =
         (size_t)(TR * F::SC + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0) + DctW4<T, FAM, LH>::N) * sizeof(typename CT<T>::C);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(row_dct_kernel<T, IT, OT, LH, R1, TR, FAM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, row_dct_kernel<T, IT, OT, LH, R1, TR, FAM>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nrows + TR - 1) / TR, ncomp);
     row_dct_kernel<T, IT, OT, LH, R1, TR, FAM><<<grid, TR * F::P, smem, s>>>(a);
     return cudaGetLastError();
@@ -1118,16 +1102,11 @@ inline cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, LH, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + RowTw<T, LH>::N) * sizeof(typename CT<T>::C);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e;
-        if constexpr (C2R)
-            e = cudaFuncSetAttribute(row_c2r_kernel<T, XT, LH, R1, TR, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        else
-            e = cudaFuncSetAttribute(row_r2c_kernel<T, XT, LH, R1, TR, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    cudaError_t e;
+    if constexpr (C2R) e = smem_attr_once(attr, row_c2r_kernel<T, XT, LH, R1, TR, HALF>, smem);
+    else e = smem_attr_once(attr, row_r2c_kernel<T, XT, LH, R1, TR, HALF>, smem);
+    if (e != cudaSuccess) return e;
     dim3 grid((a.nrows + TR - 1) / TR, ncomp);
     if constexpr (C2R) row_c2r_kernel<T, XT, LH, R1, TR, HALF><<<grid, TR * F::P, smem, s>>>(a);
     else row_r2c_kernel<T, XT, LH, R1, TR, HALF><<<grid, TR * F::P, smem, s>>>(a);

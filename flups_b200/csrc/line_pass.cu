@@ -24,6 +24,7 @@
 
 #include "cplx.cuh"
 #include "pass_desc.h"
+#include "smem_attr.cuh"
 #include "spectral.cuh"
 
 namespace flb {
@@ -460,12 +461,8 @@ size_t line_pass_smem(const PassArgs& A, int elem_bytes) {
 template <typename T>
 cudaError_t launch_line_pass_t(const PassArgs& A, int in_f64, int out_f64, cudaStream_t stream) {
     const size_t smem = line_pass_smem(A, sizeof(T));
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(line_pass_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, line_pass_kernel<T>, 227 * 1024); e != cudaSuccess) return e;
     const int ncg = A.comps_together ? A.ncomp : 1;
     int64_t nblocks;
     if (A.comps_together) nblocks = ((int64_t)A.nlines + A.lines_per_cta - 1) / A.lines_per_cta;
