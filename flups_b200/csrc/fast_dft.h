@@ -33,6 +33,7 @@ struct ColArgs {
     double normfact;
     int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
     int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
+    int64_t in_tstr, out_tstr;  // x-tiled input / output: tile (CTA) stride, 0 = x-contiguous
     Prefetch pf;            // column passes 0 / 1 along a short-stride axis
 };
 

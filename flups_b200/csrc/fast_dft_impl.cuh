@@ -361,7 +361,9 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     T* gs = reinterpret_cast<T*>(sm + TX * F::SC + F::TW_SMEM);
     if constexpr (MODE == 2) stage_green<T, L, TX>(a, gs, o);
     // lanes outside the array read its first element and drop it (no branch)
-    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+    // x-tiled arrays: column c of CTA blockIdx.x at blockIdx.x * tstr + c
+    const int64_t xin = a.in_tstr ? (int64_t)blockIdx.x * a.in_tstr + c : x;
+    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + xin + (int64_t)p * a.in_lstr
                         : reinterpret_cast<const C*>(a.in);
     const int ls = valid ? F::P * (int)a.in_lstr : 0;
     C v[R1];
@@ -403,7 +405,8 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
         F::template fft<false, true>(v, line, p, tws + zero);
     }
     if (valid) {
-        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int64_t xout = a.out_tstr ? (int64_t)blockIdx.x * a.out_tstr + c : x;
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + xout + (int64_t)p * a.out_lstr;
         const int os = F::P * (int)a.out_lstr;
 #pragma unroll
         for (int r = 0; r < NST; ++r) {

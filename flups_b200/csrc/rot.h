@@ -14,6 +14,8 @@ struct RotArgs {
     int64_t cstr;        // component stride
     int nbatch;          // ROT: groups of 3 components
     int ncomp;           // STD: components multiplied
+    int64_t tstr;        // x-tiled spectrum: x at (x / tw) * tstr + x % tw (tstr = 0: x * str[0])
+    int tw;
     MultSpec mult;       // mode 1 (STD) or 2 (ROT): Green, folds, wave-number tables, derivative order
 };
 

@@ -535,6 +535,8 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
         c.out_lstr = A.out_str[A.axis];
         c.out_ostr = A.out_str[b];
         c.out_cstr = A.out_cstr;
+        c.in_tstr = A.in_tstr;
+        c.out_tstr = A.out_tstr;
         mode = (S0.spec[0].sign > 0) ? 1 : 0;
         if (A.fused) {
             mode = 2;
@@ -600,7 +602,9 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
             auto it = tuned_tile.find(pass_key(A, f64));
             if (it != tuned_tile.end()) c.tile = it->second;
         }
-        if (prefetch && mode != 2) col_prefetch(c, f64, L, A.ncomp);
+        // an x-tiled array is laid out for the 256-thread CTA's width; no tensor map over it
+        if (c.in_tstr || c.out_tstr) c.tile = COL_TILE_256;
+        else if (prefetch && mode != 2) col_prefetch(c, f64, L, A.ncomp);
         check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
         return;
     }
@@ -739,6 +743,8 @@ void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, 
                    (double)last.n_store * A.nlines * nc * (last.out_cplx ? 2 : 1) * (out_f64 ? 8.0 : 4.0);
     if (A.fused) bytes += (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
     const int k = timed_begin(name, bytes);
+    // x-tiled arrays exist only between the register-DFT column passes of the ROT split
+    FLB_CHECK(fk == 1 || (A.in_tstr == 0 && A.out_tstr == 0), "x-tiled array outside a register-DFT column pass");
     if (fk) launch_fast(A, fk, f64, in_f64, out_f64);
     else check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
     timed_end(k);
@@ -1124,7 +1130,7 @@ void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
 // in shared memory; splitting it lets both transforms run at the DFTs' speed
 // at the price of writing and reading the spectrum once.
 bool Solver::rot_split(int nbatch) {
-    if (dry || !use_fast) return false;
+    if (dry || !use_fast || slab_dim >= 0) return false;
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const int ipl = ndim - 1;
@@ -1143,7 +1149,24 @@ bool Solver::rot_split(int nbatch) {
     const bool ok = fast_kind(F, f64, f64, f64) == 1 && fast_kind(Bk, f64, f64, f64) == 1;
     dry = keep;
     if (!ok) return false;
-    const size_t need = state_reals(ndim, nbatch) * es;
+    // The spectrum is stored x-tiled for the column passes on either side of
+    // the curl: tiles of w x-columns (one 256-thread CTA), each tile [outer][line][w],
+    // so a CTA writes (forward) and reads (inverse) one contiguous block instead
+    // of rows one plane apart.  Its size is whole tiles (w can exceed the padded
+    // row of a short line, up to 64 columns).
+    const int w = fast_col_tile_width(f64 ? 1 : 0, F.st[0].M, COL_TILE_256);
+    const int ax = p.dim, ob = (ax == 1) ? 2 : 1;
+    const int64_t ntiles = (st[ndim].n[0] + w - 1) / w;
+    int64_t tstr_spec[3];
+    tstr_spec[0] = 1;
+    tstr_spec[ax] = w;
+    tstr_spec[ob] = (int64_t)st[ndim].n[ax] * w;
+    const int64_t tile = (int64_t)st[ndim].n[ob] * st[ndim].n[ax] * w;
+    for (int d = 0; d < 3; ++d) F.out_str[d] = Bk.in_str[d] = tstr_spec[d];
+    F.out_tstr = Bk.in_tstr = tile;
+    F.out_cstr = Bk.in_cstr = ntiles * tile;
+    const size_t need = std::max(state_reals(ndim, nbatch) * es,
+                                 (size_t)(ntiles * tile) * 2 * (size_t)es * (size_t)(lda * nbatch));
     if (spec_bytes < need) {
         drop_graphs();
         if (spec_buf) cudaFree(spec_buf);
@@ -1159,7 +1182,10 @@ bool Solver::rot_split(int nbatch) {
     memset(&R, 0, sizeof(R));
     R.data = spec_buf;
     for (int d = 0; d < 3; ++d) R.n[d] = st[ndim].n[d];
-    set_strides_internal(R.str, R.cstr, st[ndim]);
+    for (int d = 0; d < 3; ++d) R.str[d] = tstr_spec[d];
+    R.cstr = ntiles * tile;
+    R.tstr = tile;
+    R.tw = w;
     R.nbatch = nbatch;
     R.mult = mult_spec(ROT);
     const double rbytes = 2.0 * (double)st[ndim].n[0] * st[ndim].n[1] * st[ndim].n[2] * 2 * es * 3 * nbatch +
