@@ -68,6 +68,7 @@ bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const
 }
 
 int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1_of(n, f64)); }
+int fast_stage_table_len_r1(int n, int r1) { return stage_table_entries(n, r1); }
 
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };

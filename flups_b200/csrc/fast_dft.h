@@ -77,11 +77,20 @@ __host__ __device__ constexpr int fast_radix1_of(int n, int f64) {
     return (n % 3 == 0) ? (f64 ? 12 : 24) : (f64 ? 16 : 32);
 }
 int fast_radix1(int f64, int n);
+// The fused pass (mode 2) of power-of-two lines in FP64 uses the FP32 first
+// radix 32: one exchange per transform instead of two, 255 registers, two
+// 128-thread CTAs per SM (4.46 vs 5.97 ms for the 1024-point fused pass at
+// 512^3); 3 x 2^k lines keep 12 (a first radix of 24 spills 184 bytes)
+__host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
+    return (mode == 2 && n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64);
+}
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix
 __host__ __device__ constexpr int fast_gcd(int a, int b) { return b == 0 ? a : fast_gcd(b, a % b); }
-// Complex entries of the later-stage twiddle table of an n-point register DFT.
+// Complex entries of the later-stage twiddle table of an n-point register DFT
+// (first radix of the default passes, or r1).
 int fast_stage_table_len(int n, int f64);
+int fast_stage_table_len_r1(int n, int r1);
 // Entry e of that table is W_M^q = exp(-2 pi i q / M); sets q and M.
 // Layout: one block of n entries per stage after the first (Ns = r1, r1*Rs, ...
 // with Rs = gcd(n/Ns, r1)); in a block, pair (b * Rs/2 + rp) * P + p (P = n/r1)

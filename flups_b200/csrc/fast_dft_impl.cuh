@@ -949,21 +949,21 @@ inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
 // the autotuner (Solver::autotune_passes) may pick the other per pass.
 template <typename T, int L, int THREADS, int MODE, int SH>
 inline cudaError_t launch_col_threads(const ColArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = fast_radix1_of(L, sizeof(T) == 8);
+    constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, MODE);
     constexpr int TX = THREADS / (L / R1);
     static_assert(TX >= 1, "tile narrower than one column");
     return launch_col_t<T, L, R1, TX, MODE, SH>(a, ncomp, s);
 }
 
-inline int col_tile_threads(int L, int tile) {
+inline int col_tile_threads(int L, int tile, bool f64_fused = false) {
     if (tile == COL_TILE_256) return 256;
     if (tile == COL_TILE_128) return 128;
-    return L == 512 ? 128 : 256;
+    return (L == 512 || f64_fused) ? 128 : 256;
 }
 
 template <typename T, int MODE, int SH>
 inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    const bool wide = col_tile_threads(L, a.tile) == 256;
+    const bool wide = col_tile_threads(L, a.tile, sizeof(T) == 8 && MODE == 2) == 256;
     switch (L) {
         case 64: return wide ? launch_col_threads<T, 64, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 64, 128, MODE, SH>(a, ncomp, s);
         case 128: return wide ? launch_col_threads<T, 128, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 128, 128, MODE, SH>(a, ncomp, s);

@@ -196,7 +196,8 @@ struct Solver {
     void compute_green();
     const void* twiddle(int M, bool f64);
     const void* twiddle_plain(int L, bool f64);   // W_L^q, q < L
-    const void* stage_table(int n, bool f64);     // later-stage twiddles of an n-point register DFT
+    // later-stage twiddles of an n-point register DFT with first radix r1 (0: the default of the precision)
+    const void* stage_table(int n, bool f64, int r1 = 0);
     int fast_kind(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64) const;  // 0 none, 1 column, 2 row
     // arguments of a fast launch, all but the twiddle tables; mode of a column pass
     void fast_args(const flb::PassArgs& A, int kind, bool in_f64, bool out_f64, flb::ColArgs& c, flb::RowArgs& r, int& mode) const;

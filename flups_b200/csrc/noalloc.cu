@@ -59,7 +59,7 @@ namespace {
 
 struct TwSlot {
     int n;        // transform length
-    int stage;    // 0: W_n^q table, 1: later-stage table of an n-point register DFT
+    int stage;    // 0: W_n^q table; r1 > 0: later-stage table of an n-point register DFT of first radix r1
     int len;      // complex entries
     size_t off;   // byte offset in the scratch array
 };
@@ -137,10 +137,11 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
 
     // twiddle tables: one per distinct (length, layout)
     std::vector<TwSlot> slots;
+    auto r1_of = [&](int n) { return fast_radix1(f64 ? 1 : 0, n); };
     auto slot_for = [&](int n, int stage) -> size_t {
         for (const TwSlot& t : slots)
             if (t.n == n && t.stage == stage) return t.off;
-        const int len = stage ? std::max(1, fast_stage_table_len(n, f64 ? 1 : 0)) : n;
+        const int len = stage ? std::max(1, fast_stage_table_len_r1(n, stage)) : n;
         TwSlot t{n, stage, len, off};
         off = align256(off + (size_t)len * 2 * es);
         slots.push_back(t);
@@ -153,20 +154,22 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
         kinds[i] = s->fast_kind(A, f64, in64, out64);
         if (kinds[i] == 0) {
             for (int sg = 0; sg <= A.fused; ++sg) slot_for(2 * A.st[sg].M, 0);
-        } else if (kinds[i] == 1 || kinds[i] == 3) {
-            slot_for(A.st[0].M, 1);
+        } else if (kinds[i] == 1) {
+            slot_for(A.st[0].M, fast_radix1_mode(A.st[0].M, f64 ? 1 : 0, A.fused ? 2 : 0));
+        } else if (kinds[i] == 3) {
+            slot_for(A.st[0].M, r1_of(A.st[0].M));
         } else if (kinds[i] == 4) {
             const LineSpec& sp = A.st[0].spec[0];
             slot_for(2 * A.st[0].M, 0);
             if (fast_dct_family(sp.kind, sp.n_in, A.st[0].M)) {
                 slot_for(sp.n_in, 0);
-                slot_for(sp.n_in / 2, 1);
+                slot_for(sp.n_in / 2, r1_of(sp.n_in / 2));
             } else {
-                slot_for(A.st[0].M, 1);
+                slot_for(A.st[0].M, r1_of(A.st[0].M));
             }
         } else {
             slot_for(A.st[0].M, 0);
-            slot_for(A.st[0].M / 2, 1);
+            slot_for(A.st[0].M / 2, r1_of(A.st[0].M / 2));
         }
     }
     if (off > FLUPS_NOALLOC_SCRATCH_BYTES) {
@@ -179,7 +182,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     cudaStream_t st = s->stream;
     for (const TwSlot& t : slots) {
         const int nb = std::min(1184, (t.len + 255) / 256);
-        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, fast_radix1(f64 ? 1 : 0, t.n), f64 ? 1 : 0);
+        noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, t.stage, f64 ? 1 : 0);
     }
     auto tw_of = [&](int n, int stage) { return (const void*)(base + slot_for(n, stage)); };
     for (size_t i = 0; i < passes.size(); ++i) {
@@ -196,23 +199,23 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             int mode = 0;
             s->fast_args(A, kinds[i], in64, out64, c, r, mode);
             if (kinds[i] == 1) {
-                c.tws = tw_of(L, 1);
+                c.tws = tw_of(L, fast_radix1_mode(L, f64 ? 1 : 0, mode));
                 e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
             } else if (kinds[i] == 3) {
-                c.tws = tw_of(L, 1);
+                c.tws = tw_of(L, r1_of(L));
                 e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
             } else if (kinds[i] == 4) {
                 r.tw2 = tw_of(2 * L, 0);
                 if (fast_dct_family(r.kind, r.n, L)) {
                     r.tw = tw_of(r.n, 0);
-                    r.tws = tw_of(r.n / 2, 1);
+                    r.tws = tw_of(r.n / 2, r1_of(r.n / 2));
                 } else {
-                    r.tws = tw_of(L, 1);
+                    r.tws = tw_of(L, r1_of(L));
                 }
                 e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
             } else {
                 r.tw = tw_of(L, 0);
-                r.tws = tw_of(L / 2, 1);
+                r.tws = tw_of(L / 2, r1_of(L / 2));
                 e = launch_fast_row(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, st);
             }
         }

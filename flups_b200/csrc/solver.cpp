@@ -595,7 +595,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         return;
     }
     if (kind == 1) {
-        c.tws = stage_table(L, f64);
+        c.tws = stage_table(L, f64, fast_radix1_mode(L, f64 ? 1 : 0, mode));
         if (force_tile) {
             c.tile = force_tile;
         } else if (!tuned_tile.empty()) {
@@ -651,11 +651,12 @@ void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) cons
     make_prefetch(r.pf, r.in, dims, strides, box, (int)((units + 255) / 256), 256, PREFETCH_DIST);
 }
 
-const void* Solver::stage_table(int n, bool f64) {
-    const int64_t key = ((int64_t)1 << 40) + (int64_t)n * 2 + (f64 ? 1 : 0);
+const void* Solver::stage_table(int n, bool f64, int r1) {
+    if (r1 == 0) r1 = fast_radix1(f64 ? 1 : 0, n);
+    const int64_t key = ((int64_t)1 << 40) + ((int64_t)r1 << 32) + (int64_t)n * 2 + (f64 ? 1 : 0);
     auto it = twiddles.find(key);
     if (it != twiddles.end()) return it->second;
-    const int len = fast_stage_table_len(n, f64 ? 1 : 0), r1 = fast_radix1(f64 ? 1 : 0, n);
+    const int len = fast_stage_table_len_r1(n, r1);
     std::vector<double> w(2 * (size_t)std::max(len, 1), 0.0);
     for (int e = 0; e < len; ++e) {
         int q = 0, M = 1;
@@ -1627,7 +1628,7 @@ void Solver::autotune_passes(int type, int nbatch) {
         int mode = 0;
         fast_args(A, 1, f64, f64, c, r, mode);
         const int L = A.st[0].M;
-        c.tws = stage_table(L, f64);
+        c.tws = stage_table(L, f64, fast_radix1_mode(L, f64 ? 1 : 0, mode));
         float best = 1e30f;
         int best_tile = COL_TILE_DEFAULT;
         for (int tile : {COL_TILE_256, COL_TILE_128}) {
