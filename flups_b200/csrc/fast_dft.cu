@@ -25,7 +25,9 @@ bool fast_row_supported(int L) {
 
 int fast_radix1(int f64, int n) { return fast_radix1_of(n, f64); }
 
-int fast_col_tile_width(int f64, int L, int tile) { return col_tile_threads(L, tile) / (L / fast_radix1_of(L, f64)); }
+int fast_col_tile_width(int f64, int L, int tile) {
+    return col_tile_threads(L, tile, f64 && L % 3 != 0) / (L / fast_radix1_mode(L, f64, 0));
+}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library)

@@ -67,7 +67,7 @@ bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const
                    int nbox, int step, int dist);
 
 bool fast_col_supported(int L);
-// columns per CTA of a column pass of length L with CTA tile `tile`
+// columns per CTA of a column c2c pass of length L with CTA tile `tile`
 int fast_col_tile_width(int f64, int L, int tile);
 bool fast_row_supported(int L);
 
@@ -77,12 +77,13 @@ __host__ __device__ constexpr int fast_radix1_of(int n, int f64) {
     return (n % 3 == 0) ? (f64 ? 12 : 24) : (f64 ? 16 : 32);
 }
 int fast_radix1(int f64, int n);
-// The fused pass (mode 2) of power-of-two lines in FP64 uses the FP32 first
-// radix 32: one exchange per transform instead of two, 255 registers, two
-// 128-thread CTAs per SM (4.46 vs 5.97 ms for the 1024-point fused pass at
-// 512^3); 3 x 2^k lines keep 12 (a first radix of 24 spills 184 bytes)
+// The column passes (modes 0, 1, 2) of power-of-two lines in FP64 use the FP32
+// first radix 32: one exchange per transform instead of two, up to 255
+// registers, two 128-thread CTAs per SM (512^3: fused 5.97 -> 4.47 ms, y
+// forward 1.57 -> 1.24 ms, y inverse 1.65 -> 1.37 ms); 3 x 2^k lines keep 12
+// (a first radix of 24 spills 184 bytes).  `mode` is kept for the callers.
 __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
-    return (mode == 2 && n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64);
+    return (mode >= 0 && n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64);
 }
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix

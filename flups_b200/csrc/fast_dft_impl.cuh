@@ -320,15 +320,15 @@ __device__ __forceinline__ void stage_green(const ColArgs& a, T* gs, int o) {
 #ifndef FLB_FUSED_THREADS_PER_SM
 #define FLB_FUSED_THREADS_PER_SM 512
 #endif
-// the FP64 fused pass holds its twiddles and Green's values in registers
-// (225 per thread) instead of spilling at 128: one 256-thread CTA per SM
-// measured 5.98 vs 6.18 ms at 512^3
-#ifndef FLB_FUSED_F64_THREADS_PER_SM
-#define FLB_FUSED_F64_THREADS_PER_SM 256
+// FP64 column passes with a first radix of 32 (and every FP64 fused pass) hold
+// 16-32 complex doubles and their twiddles in registers: 256 threads per SM,
+// up to 255 registers each, instead of spilling at 128
+#ifndef FLB_F64_WIDE_THREADS_PER_SM
+#define FLB_F64_WIDE_THREADS_PER_SM 256
 #endif
-template <int THREADS, bool FUSED = false, bool F64 = false>
+template <int THREADS, bool FUSED = false, bool F64_WIDE = false>
 struct Occ {
-    static constexpr int per_sm = FUSED ? (F64 ? FLB_FUSED_F64_THREADS_PER_SM : FLB_FUSED_THREADS_PER_SM) : FLB_COL_THREADS_PER_SM;
+    static constexpr int per_sm = F64_WIDE ? FLB_F64_WIDE_THREADS_PER_SM : (FUSED ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM);
     static constexpr int want = per_sm / (THREADS < 64 ? 64 : THREADS);
     static constexpr int blocks = want < 1 ? 1 : want;
 };
@@ -341,7 +341,7 @@ enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
 //      2: forward, Green multiply, inverse (SH: loaded and stored part).
 // The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
 template <typename T, int L, int R1, int TX, int MODE, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, sizeof(T) == 8>::blocks)) col_dft_kernel(const __grid_constant__ ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, sizeof(T) == 8 && (MODE == 2 || R1 == 32)>::blocks)) col_dft_kernel(const __grid_constant__ ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
@@ -945,8 +945,10 @@ inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
 
 // CTA tiles of a column pass: THREADS threads = TX columns x P threads per
 // line.  Two tiles are compiled per length (256 and 128 threads); the default
-// is 256 threads except at L = 512, where 128 threads (8 FP32 columns) won;
-// the autotuner (Solver::autotune_passes) may pick the other per pass.
+// is 256 threads except at L = 512, where 128 threads (8 FP32 columns) won,
+// and for the FP64 passes at 255 registers (first radix 32, or fused), which
+// run two 128-thread CTAs per SM; the autotuner (Solver::autotune_passes) may
+// pick the other per pass.
 template <typename T, int L, int THREADS, int MODE, int SH>
 inline cudaError_t launch_col_threads(const ColArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, MODE);
@@ -955,15 +957,17 @@ inline cudaError_t launch_col_threads(const ColArgs& a, int ncomp, cudaStream_t 
     return launch_col_t<T, L, R1, TX, MODE, SH>(a, ncomp, s);
 }
 
-inline int col_tile_threads(int L, int tile, bool f64_fused = false) {
+// default: 128 threads at L = 512 and for the FP64 passes at 255 registers
+// (two CTAs per SM), else 256
+inline int col_tile_threads(int L, int tile, bool prefer128 = false) {
     if (tile == COL_TILE_256) return 256;
     if (tile == COL_TILE_128) return 128;
-    return (L == 512 || f64_fused) ? 128 : 256;
+    return (L == 512 || prefer128) ? 128 : 256;
 }
 
 template <typename T, int MODE, int SH>
 inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    const bool wide = col_tile_threads(L, a.tile, sizeof(T) == 8 && MODE == 2) == 256;
+    const bool wide = col_tile_threads(L, a.tile, sizeof(T) == 8 && (MODE == 2 || L % 3 != 0)) == 256;
     switch (L) {
         case 64: return wide ? launch_col_threads<T, 64, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 64, 128, MODE, SH>(a, ncomp, s);
         case 128: return wide ? launch_col_threads<T, 128, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 128, 128, MODE, SH>(a, ncomp, s);
