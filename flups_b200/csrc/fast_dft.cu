@@ -25,6 +25,12 @@ bool fast_row_supported(int L) {
 
 int fast_radix1(int f64, int n) { return fast_radix1_of(n, f64); }
 
+int fast_row_tile_rows(int f64, int L) {
+    const int lh = L / 2, r1 = fast_radix1_row(lh, f64), p = lh / r1;
+    const int threads = (f64 && r1 == 32) ? 128 : 256;
+    return p >= threads ? 1 : threads / p;
+}
+
 int fast_col_tile_width(int f64, int L, int tile) {
     return col_tile_threads(L, tile, f64 && L % 3 != 0) / (L / fast_radix1_mode(L, f64, 0));
 }

@@ -69,6 +69,8 @@ bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const
 bool fast_col_supported(int L);
 // columns per CTA of a column c2c pass of length L with CTA tile `tile`
 int fast_col_tile_width(int f64, int L, int tile);
+// rows per CTA of the r2c / c2r row pass of real length L
+int fast_row_tile_rows(int f64, int L);
 bool fast_row_supported(int L);
 
 // First radix of the register DFTs for an n-point line: 32 in FP32 and 16 in
@@ -77,6 +79,11 @@ __host__ __device__ constexpr int fast_radix1_of(int n, int f64) {
     return (n % 3 == 0) ? (f64 ? 12 : 24) : (f64 ? 16 : 32);
 }
 int fast_radix1(int f64, int n);
+// first radix of the r2c / c2r rows (half-length DFT of n points): the FP64
+// rows of power-of-two lines use 32 like the columns below
+__host__ __device__ constexpr int fast_radix1_row(int n, int f64) {
+    return (f64 && n % 3 != 0) ? 32 : fast_radix1_of(n, f64);
+}
 // The column passes (modes 0, 1, 2) of power-of-two lines in FP64 use the FP32
 // first radix 32: one exchange per transform instead of two, up to 255
 // registers, two 128-thread CTAs per SM (512^3: fused 5.97 -> 4.47 ms, y

@@ -491,6 +491,16 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) c
     }
 }
 
+// rows per CTA of the r2c / c2r row kernels: 256 threads, or 128 for the FP64
+// rows with a first radix of 32 (255 registers, two CTAs per SM)
+template <typename T, int LH, int R1>
+struct RowTiles {
+    static constexpr bool WIDE = sizeof(T) == 8 && R1 == 32;
+    static constexpr int P = LH / R1;
+    static constexpr int THREADS = WIDE ? 128 : 256;
+    static constexpr int TR = (P >= THREADS) ? 1 : THREADS / P;
+};
+
 // ---------------------------------------------------------------- rows: r2c
 template <typename IT> struct Vec2;
 template <> struct Vec2<float> { using V = float2; };
@@ -499,7 +509,7 @@ template <> struct Vec2<double> { using V = double2; };
 // IT: type of the real input (the user's double array, or the working precision);
 // HALF: nin = Lh (the row is zero-padded to twice its length)
 template <typename T, typename IT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_r2c_kernel(const __grid_constant__ RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE>::blocks)) row_r2c_kernel(const __grid_constant__ RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     using V = typename Vec2<IT>::V;
@@ -848,7 +858,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
 // ---------------------------------------------------------------- rows: c2r
 // OT: type of the real output; HALF: nout = Lh (the row is truncated to half)
 template <typename T, typename OT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), Occ<TR * (LH / R1)>::blocks) row_c2r_kernel(const __grid_constant__ RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE>::blocks)) row_c2r_kernel(const __grid_constant__ RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     using V = typename Vec2<OT>::V;
@@ -1107,7 +1117,7 @@ inline cudaError_t launch_dct_types(int f64, int in64, int out64, int n, const R
 template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
 inline cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, LH, R1, true>;
-    constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
+    constexpr int TR = RowTiles<T, LH, R1>::TR;
     const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + RowTw<T, LH>::N) * sizeof(typename CT<T>::C);
     static std::atomic<unsigned long long> attr{0};
     cudaError_t e;
@@ -1124,20 +1134,20 @@ template <typename T, typename XT, bool C2R, bool HALF>
 inline cudaError_t launch_row_len(int L, const RowArgs& a, int ncomp, cudaStream_t s) {
     constexpr bool F64 = sizeof(T) == 8;
     switch (L) {
-        case 128: return launch_row_t<T, XT, 64, fast_radix1_of(64, F64), C2R, HALF>(a, ncomp, s);
-        case 256: return launch_row_t<T, XT, 128, fast_radix1_of(128, F64), C2R, HALF>(a, ncomp, s);
-        case 512: return launch_row_t<T, XT, 256, fast_radix1_of(256, F64), C2R, HALF>(a, ncomp, s);
-        case 1024: return launch_row_t<T, XT, 512, fast_radix1_of(512, F64), C2R, HALF>(a, ncomp, s);
-        case 2048: return launch_row_t<T, XT, 1024, fast_radix1_of(1024, F64), C2R, HALF>(a, ncomp, s);
-        case 4096: return launch_row_t<T, XT, 2048, fast_radix1_of(2048, F64), C2R, HALF>(a, ncomp, s);
-        case 48: return launch_row_t<T, XT, 24, fast_radix1_of(24, F64), C2R, HALF>(a, ncomp, s);
-        case 64: return launch_row_t<T, XT, 32, fast_radix1_of(32, F64), C2R, HALF>(a, ncomp, s);
-        case 96: return launch_row_t<T, XT, 48, fast_radix1_of(48, F64), C2R, HALF>(a, ncomp, s);
-        case 192: return launch_row_t<T, XT, 96, fast_radix1_of(96, F64), C2R, HALF>(a, ncomp, s);
-        case 384: return launch_row_t<T, XT, 192, fast_radix1_of(192, F64), C2R, HALF>(a, ncomp, s);
-        case 768: return launch_row_t<T, XT, 384, fast_radix1_of(384, F64), C2R, HALF>(a, ncomp, s);
-        case 1536: return launch_row_t<T, XT, 768, fast_radix1_of(768, F64), C2R, HALF>(a, ncomp, s);
-        case 3072: return launch_row_t<T, XT, 1536, fast_radix1_of(1536, F64), C2R, HALF>(a, ncomp, s);
+        case 128: return launch_row_t<T, XT, 64, fast_radix1_row(64, F64), C2R, HALF>(a, ncomp, s);
+        case 256: return launch_row_t<T, XT, 128, fast_radix1_row(128, F64), C2R, HALF>(a, ncomp, s);
+        case 512: return launch_row_t<T, XT, 256, fast_radix1_row(256, F64), C2R, HALF>(a, ncomp, s);
+        case 1024: return launch_row_t<T, XT, 512, fast_radix1_row(512, F64), C2R, HALF>(a, ncomp, s);
+        case 2048: return launch_row_t<T, XT, 1024, fast_radix1_row(1024, F64), C2R, HALF>(a, ncomp, s);
+        case 4096: return launch_row_t<T, XT, 2048, fast_radix1_row(2048, F64), C2R, HALF>(a, ncomp, s);
+        case 48: return launch_row_t<T, XT, 24, fast_radix1_row(24, F64), C2R, HALF>(a, ncomp, s);
+        case 64: return launch_row_t<T, XT, 32, fast_radix1_row(32, F64), C2R, HALF>(a, ncomp, s);
+        case 96: return launch_row_t<T, XT, 48, fast_radix1_row(48, F64), C2R, HALF>(a, ncomp, s);
+        case 192: return launch_row_t<T, XT, 96, fast_radix1_row(96, F64), C2R, HALF>(a, ncomp, s);
+        case 384: return launch_row_t<T, XT, 192, fast_radix1_row(192, F64), C2R, HALF>(a, ncomp, s);
+        case 768: return launch_row_t<T, XT, 384, fast_radix1_row(384, F64), C2R, HALF>(a, ncomp, s);
+        case 1536: return launch_row_t<T, XT, 768, fast_radix1_row(768, F64), C2R, HALF>(a, ncomp, s);
+        case 3072: return launch_row_t<T, XT, 1536, fast_radix1_row(1536, F64), C2R, HALF>(a, ncomp, s);
     }
     return cudaErrorInvalidValue;
 }

@@ -169,7 +169,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             }
         } else {
             slot_for(A.st[0].M, 0);
-            slot_for(A.st[0].M / 2, r1_of(A.st[0].M / 2));
+            slot_for(A.st[0].M / 2, fast_radix1_row(A.st[0].M / 2, f64 ? 1 : 0));
         }
     }
     if (off > FLUPS_NOALLOC_SCRATCH_BYTES) {
@@ -215,7 +215,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                 e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
             } else {
                 r.tw = tw_of(L, 0);
-                r.tws = tw_of(L / 2, r1_of(L / 2));
+                r.tws = tw_of(L / 2, fast_radix1_row(L / 2, f64 ? 1 : 0));
                 e = launch_fast_row(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, st);
             }
         }

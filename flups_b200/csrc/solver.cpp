@@ -609,7 +609,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         return;
     }
     r.tw = twiddle_plain(L, f64);
-    r.tws = stage_table(L / 2, f64);
+    r.tws = stage_table(L / 2, f64, fast_radix1_row(L / 2, f64 ? 1 : 0));
     const bool c2r = A.st[0].spec[0].kind == LK_C2R;
     if (prefetch) row_prefetch(r, f64, c2r, L, A.ncomp);
     check_cuda(launch_fast_row(f64, c2r, L, r, A.ncomp, stream), "row DFT launch");
@@ -641,8 +641,7 @@ void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) cons
     const uint64_t row_bytes = (uint64_t)r.nin * elem;
     if ((double)row_bytes * r.nrows * ncomp < PREFETCH_MIN_BYTES) return;
     const uint64_t units = (row_bytes + 7) / 8;
-    const int p = lh / fast_radix1(f64 ? 1 : 0, lh);
-    const int tr = p >= 256 ? 1 : 256 / p;
+    const int tr = fast_row_tile_rows(f64 ? 1 : 0, L);
     const uint64_t n2 = (uint64_t)(r.nrows / r.n1);
     const uint64_t s2 = (uint64_t)r.in_s2 * elem;
     const uint64_t dims[4] = {units, (uint64_t)r.n1, n2, (uint64_t)ncomp};
