@@ -367,6 +367,81 @@ template <bool INV = false, bool Z = false, typename C> __device__ __forceinline
     for (int i = 0; i < 24; ++i) v[i] = t[i];
 }
 
+// W48^m = (cos(pi m/24), -sin(pi m/24)) for the m = n1*k2 products of dft48
+template <typename S> __device__ __forceinline__ void w48(int m, S& c, S& s) {
+    switch (m) {
+        case 1: c = (S)0.9914448613738104111446; s = -(S)0.1305261922200515915484; break;
+        case 2: c = (S)0.9659258262890682867497; s = -(S)0.2588190451025207623489; break;
+        case 3: c = (S)0.9238795325112867561282; s = -(S)0.3826834323650897717285; break;
+        case 4: c = (S)0.8660254037844386467637; s = -(S)0.5000000000000000000000; break;
+        case 5: c = (S)0.7933533402912351645798; s = -(S)0.6087614290087206394161; break;
+        case 6: c = (S)0.7071067811865475244008; s = -(S)0.7071067811865475244008; break;
+        case 7: c = (S)0.6087614290087206394161; s = -(S)0.7933533402912351645798; break;
+        case 8: c = (S)0.5000000000000000000000; s = -(S)0.8660254037844386467637; break;
+        case 9: c = (S)0.3826834323650897717285; s = -(S)0.9238795325112867561282; break;
+        case 10: c = (S)0.2588190451025207623489; s = -(S)0.9659258262890682867497; break;
+        case 11: c = (S)0.1305261922200515915484; s = -(S)0.9914448613738104111446; break;
+        case 13: c = -(S)0.1305261922200515915484; s = -(S)0.9914448613738104111446; break;
+        case 14: c = -(S)0.2588190451025207623489; s = -(S)0.9659258262890682867497; break;
+        case 15: c = -(S)0.3826834323650897717285; s = -(S)0.9238795325112867561282; break;
+        case 16: c = -(S)0.5000000000000000000000; s = -(S)0.8660254037844386467637; break;
+        case 17: c = -(S)0.6087614290087206394161; s = -(S)0.7933533402912351645798; break;
+        case 18: c = -(S)0.7071067811865475244008; s = -(S)0.7071067811865475244008; break;
+        case 19: c = -(S)0.7933533402912351645798; s = -(S)0.6087614290087206394161; break;
+        case 20: c = -(S)0.8660254037844386467637; s = -(S)0.5000000000000000000000; break;
+        case 21: c = -(S)0.9238795325112867561282; s = -(S)0.3826834323650897717285; break;
+        case 22: c = -(S)0.9659258262890682867497; s = -(S)0.2588190451025207623489; break;
+        case 23: c = -(S)0.9914448613738104111446; s = -(S)0.1305261922200515915484; break;
+        case 24: c = (S)-1; s = (S)0; break;
+        case 25: c = -(S)0.9914448613738104111446; s = (S)0.1305261922200515915484; break;
+        case 26: c = -(S)0.9659258262890682867497; s = (S)0.2588190451025207623489; break;
+        case 27: c = -(S)0.9238795325112867561282; s = (S)0.3826834323650897717285; break;
+        case 28: c = -(S)0.8660254037844386467637; s = (S)0.5000000000000000000000; break;
+        case 29: c = -(S)0.7933533402912351645798; s = (S)0.6087614290087206394161; break;
+        case 30: c = -(S)0.7071067811865475244008; s = (S)0.7071067811865475244008; break;
+        default: c = (S)1; s = (S)0; break;
+    }
+}
+
+// DFT48 as 3 x 16: inner DFT16 over n2 of a[n1 + 3 n2], twiddle W48^{n1 k2},
+// outer DFT3 over n1; output k2 + 16 k1.  Z: inputs 24..47 are zero (then the
+// inner DFT16s see a zero upper half).
+template <bool INV = false, bool Z = false, typename C> __device__ __forceinline__ void dft48(C* v) {
+    using S = decltype(v[0].x);
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) {
+        C a[16];
+#pragma unroll
+        for (int n2 = 0; n2 < 16; ++n2) a[n2] = v[n1 + 3 * n2];
+        if constexpr (Z) dft16z(a);
+        else dft16<INV>(a);
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) v[n1 + 3 * k2] = a[k2];
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < 3; ++n1) {
+#pragma unroll
+        for (int k2 = 1; k2 < 16; ++k2) {
+            if (n1 * k2 == 12) {
+                v[n1 + 3 * k2] = INV ? cmul_pi(v[n1 + 3 * k2]) : cmul_mi(v[n1 + 3 * k2]);
+            } else {
+                S c, s;
+                w48<S>(n1 * k2, c, s);
+                v[n1 + 3 * k2] = cmul(v[n1 + 3 * k2], mkc(c, INV ? -s : s));
+            }
+        }
+    }
+    C t[48];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        C a0 = v[3 * k2], a1 = v[1 + 3 * k2], a2 = v[2 + 3 * k2];
+        dft3<INV>(a0, a1, a2);
+        t[k2] = a0; t[k2 + 16] = a1; t[k2 + 32] = a2;
+    }
+#pragma unroll
+    for (int i = 0; i < 48; ++i) v[i] = t[i];
+}
+
 // W12^m = (cos(pi m/6), -sin(pi m/6))
 template <typename S> __device__ __forceinline__ void w12(int m, S& c, S& s) {
     switch (m) {

@@ -32,7 +32,8 @@ int fast_row_tile_rows(int f64, int L) {
 }
 
 int fast_col_tile_width(int f64, int L, int tile) {
-    return col_tile_threads(L, tile, f64 && L % 3 != 0) / (L / fast_radix1_mode(L, f64, 0));
+    const int r1 = fast_radix1_mode(L, f64, 0);
+    return col_tile_threads(L, tile, (f64 && L % 3 != 0) || r1 == 48) / (L / r1);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link

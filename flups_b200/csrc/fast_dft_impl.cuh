@@ -40,6 +40,7 @@ __device__ __forceinline__ void dftr(C* v) {
     else if constexpr (R == 32) dft32<INV>(v);
     else if constexpr (R == 24) dft24<INV>(v);
     else if constexpr (R == 12) dft12<INV>(v);
+    else if constexpr (R == 48) dft48<INV>(v);
 }
 
 // radix-R DFT of v whose upper half is zero
@@ -52,6 +53,7 @@ __device__ __forceinline__ void dftz(C* v) {
     else if constexpr (R == 32) dft32z(v);
     else if constexpr (R == 24) dft24<false, true>(v);
     else if constexpr (R == 12) dft12<false, true>(v);
+    else if constexpr (R == 48) dft48<false, true>(v);
 }
 
 // two consecutive complex twiddles of a stage table, from shared memory
@@ -977,7 +979,8 @@ inline int col_tile_threads(int L, int tile, bool prefer128 = false) {
 
 template <typename T, int MODE, int SH>
 inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    const bool wide = col_tile_threads(L, a.tile, sizeof(T) == 8 && (MODE == 2 || L % 3 != 0)) == 256;
+    const bool wide =
+        col_tile_threads(L, a.tile, (sizeof(T) == 8 && (MODE == 2 || L % 3 != 0)) || fast_radix1_mode(L, sizeof(T) == 8, MODE) == 48) == 256;
     switch (L) {
         case 64: return wide ? launch_col_threads<T, 64, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 64, 128, MODE, SH>(a, ncomp, s);
         case 128: return wide ? launch_col_threads<T, 128, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 128, 128, MODE, SH>(a, ncomp, s);

@@ -103,3 +103,34 @@ def test_spectral_filter_like_the_sample():
     k2 = 3 * (2 * np.pi) ** 2
     exact = -np.exp(-sig * k2) / k2 * u
     assert np.linalg.norm(out - exact) / np.linalg.norm(exact) <= 1e-12
+
+
+@pytest.mark.parametrize("nglob,precision", [([32, 384, 32], 32), ([384, 32, 32], 32), ([32, 384, 32], 64),
+                                             ([48, 40, 36], 32), ([64] * 3, 64)])
+def test_forward_spectrum_matches_numpy(nglob, precision):
+    """The forward transforms alone (flups_do_FFT) against numpy: an all-unbounded
+    cell-centred field is zero-padded to twice its size and transformed (r2c in
+    x, c2c in y and z).  Unlike a solve, this checks each transform on its own,
+    so an error that a forward / inverse pair would undo cannot hide (768-point
+    lines: first radix 48 in FP32 rows and columns)."""
+    nx, ny, nz = nglob
+    h = [1.0 / nx] * 3
+    t, s = make_solver(nglob, 1, [[[4], [4]]] * 3, h, [h[d] * nglob[d] for d in range(3)], CELL_CENTER, HEJ_2,
+                       precision=precision)
+    f = np.random.default_rng(7).standard_normal((nx, ny, nz))
+    u = to_user(f[None])
+    inner = s.get_inner_buffer()
+    s.do_copy(t, u, FWD)
+    s.do_fft(inner, FWD)
+    ts = s.get_inner_topo_spectral()
+    nmem = [ts.get_nmem(d) for d in range(3)]
+    nloc = [ts.get_nloc(d) for d in range(3)]
+    assert nloc == [nx + 1, 2 * ny, 2 * nz]
+    view = inner[: 2 * nmem[0] * nmem[1] * nmem[2]].reshape(nmem[2], nmem[1], nmem[0], 2)
+    got = view[: nloc[2], : nloc[1], : nloc[0], 0] + 1j * view[: nloc[2], : nloc[1], : nloc[0], 1]
+    a = np.zeros((2 * nz, 2 * ny, 2 * nx))
+    a[:nz, :ny, :nx] = f.transpose(2, 1, 0)
+    ref = np.fft.fft(np.fft.fft(np.fft.rfft(a, axis=2), axis=1), axis=0)
+    tol = 2e-6 if precision == 32 else 1e-12
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= tol
+    assert s.last_error() == 0

@@ -71,6 +71,9 @@ CASES = [
     ("node_oe_per_unb65_dst23", [65, 33, 33], 1, [[[1], [0]], [[3], [3]], [[4], [4]]], NODE_CENTER, CHAT_2),
     ("vector3_eopu64_dct4", [64, 32, 32], 3, [[[0, 0, 0], [1, 1, 1]], [[3] * 3, [3] * 3], [[4] * 3, [4] * 3]],
      CELL_CENTER, HEJ_2),
+    # 768-point lines: FP32 first radix 48 (two stages) in the x rows (half length 384) and the y columns
+    ("unb_384x32x32_r48", [384, 32, 32], 1, UNB3, CELL_CENTER, HEJ_2),
+    ("unb_32x384x32_r48", [32, 384, 32], 1, UNB3, CELL_CENTER, LGF_2),
     # node EVEN/EVEN x: DCT-I rows through the extended-row DFT
     ("node_ee_unb65_dct1", [65, 33, 33], 1, [[[0], [0]], [[4], [4]], [[4], [4]]], NODE_CENTER, CHAT_2),
 ]
@@ -81,6 +84,16 @@ def test_fast_fp64_matches_oracle(name, nglob, lda, bcv, center, kernel):
     got, ref, plan = _run(nglob, lda, bcv, center, kernel, 64, True)
     assert any(p["fast"] for p in plan["passes"] if p["name"] != "green"), "fast kernels not selected"
     assert rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("name,nglob", [(c[0], c[1]) for c in CASES if c[0].endswith("_r48")])
+def test_radix48_lines_run_the_register_dft(name, nglob):
+    """The 768-point lines of the radix-48 cases run the register DFT (not the
+    general line pass) in FP32, so the parity cases above check that path."""
+    case = next(c for c in CASES if c[0] == name)
+    _, _, plan = _run(case[1], case[2], case[3], case[4], case[5], 32, True)
+    long_passes = [p for p in plan["passes"] if p["name"] != "green" and p["st"][0]["M"] == 768]
+    assert long_passes and all(p["fast"] for p in long_passes), long_passes
 
 
 @pytest.mark.parametrize("name,nglob,lda,bcv,center,kernel", CASES, ids=[c[0] for c in CASES])
