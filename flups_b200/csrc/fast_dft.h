@@ -79,22 +79,24 @@ __host__ __device__ constexpr int fast_radix1_of(int n, int f64) {
     return (n % 3 == 0) ? (f64 ? 12 : 24) : (f64 ? 16 : 32);
 }
 int fast_radix1(int f64, int n);
-// first radix of the r2c / c2r rows (half-length DFT of n points): the FP64
-// rows of power-of-two lines use 32 like the columns below
-// first radix 48 (3 x 16) for the FP32 384- and 768-point lines of the forward /
-// inverse columns and the rows: two Stockham stages instead of three (768-point
-// columns 0.62 -> 0.56 ms along y, 0.87 -> 0.72 ms along z at 384^3)
+// First radices that differ from fast_radix1_of (the tables of those passes
+// are built with the same functions):
+//  - FP32 384- and 768-point lines of the forward / inverse columns and the
+//    rows: 48 (3 x 16), two Stockham stages instead of three (768-point
+//    columns 0.62 -> 0.56 ms along y, 0.87 -> 0.72 ms along z at 384^3);
+//  - FP64 power-of-two lines of the column passes (modes 0, 1, 2) and of the
+//    rows: 32, one exchange per transform instead of two, up to 255 registers
+//    in two 128-thread CTAs per SM (512^3: fused 5.97 -> 4.47 ms, y passes
+//    1.57 / 1.65 -> 1.24 / 1.37 ms in a standalone driver); 3 x 2^k lines keep
+//    12 (a first radix of 24 spills 184 bytes in the fused pass).
 __host__ __device__ constexpr bool fast_radix48(int n, int f64) { return !f64 && (n == 384 || n == 768); }
+// rows: n is the half-length DFT of the r2c / c2r split
 __host__ __device__ constexpr int fast_radix1_row(int n, int f64) {
     return fast_radix48(n, f64) ? 48 : ((f64 && n % 3 != 0) ? 32 : fast_radix1_of(n, f64));
 }
-// The column passes (modes 0, 1, 2) of power-of-two lines in FP64 use the FP32
-// first radix 32: one exchange per transform instead of two, up to 255
-// registers, two 128-thread CTAs per SM (512^3: fused 5.97 -> 4.47 ms, y
-// forward 1.57 -> 1.24 ms, y inverse 1.65 -> 1.37 ms); 3 x 2^k lines keep 12
-// (a first radix of 24 spills 184 bytes).  `mode` is kept for the callers.
+// column c2c passes of mode 0 (forward), 1 (inverse) or 2 (fused: radix 48 not used)
 __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
-    return (mode != 2 && fast_radix48(n, f64)) ? 48 : ((mode >= 0 && n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
+    return (mode != 2 && fast_radix48(n, f64)) ? 48 : ((n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
 }
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix

@@ -636,7 +636,6 @@ void Solver::col_prefetch(ColArgs& c, bool f64, int L, int ncomp) const {
 }
 
 void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) const {
-    const int lh = L / 2;
     const int elem = c2r ? (f64 ? 16 : 8) : (r.in_f64 ? 8 : 4);
     const uint64_t row_bytes = (uint64_t)r.nin * elem;
     if ((double)row_bytes * r.nrows * ncomp < PREFETCH_MIN_BYTES) return;
