@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "config2", "config3"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "node513", "rot384"],
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
@@ -329,7 +329,7 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def config2_rhs(dev):
+def node513_rhs(dev):
     """513 x 257 x 257 nodes at i h (h = 1/256) on [0,2]x[0,1]x[0,1]: sum of 8 Gaussians,
     centres uniform in the domain shrunk by 0.2 L per side, sigma in [0.03,0.08], a in [-1,1]."""
     import torch
@@ -348,7 +348,7 @@ def config2_rhs(dev):
     return f
 
 
-def config3_rhs(n, dev):
+def vortex_ring_rhs(n, dev):
     """Vortex ring on n^3 cells of [0,1]^3: centre (0.5,0.5,0.5), axis z, radius
     R(theta) = 0.25 (1 + sum_{m=1..8} a_m cos(m theta + phi_m)), a_m in [-1e-3,1e-3],
     phi_m in [0,2 pi); azimuthal vorticity Gamma/(pi s^2) exp(-d^2/s^2), Gamma = 1,
@@ -382,8 +382,8 @@ def fast_flags(stats, plan):
 
 
 def run_config(args):
-    """Config 2 (node-centred 513x257x257, EVEN/ODD x, PER y, UNB z, HEJ_4) or
-    config 3 (384^3 cell, all UNB, LGF_4, ROT with the spectral curl, 3 components):
+    """node513 (node-centred 513x257x257, EVEN/ODD x, PER y, UNB z, HEJ_4) or
+    rot384 (384^3 cell, all UNB, LGF_4, ROT with the spectral curl, 3 components):
     FP32 and FP64 solves of device arrays, the FP32 error against the FP64 mode,
     and the per-pass times (which show the general line-pass kernel where the
     register DFTs do not apply)."""
@@ -393,19 +393,19 @@ def run_config(args):
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
     B = pf.BoundaryType
-    if args.workload == "config2":
+    if args.workload == "node513":
         nglob, lda, typ = [513, 257, 257], 1, 0
         bcs = [[B.EVEN, B.ODD], [B.PER, B.PER], [B.UNB, B.UNB]]
         h, L, center, kernel, odiff = [1 / 256] * 3, [2.0, 1.0, 1.0], pf.CenterType.NODE_CENTER, "HEJ_4", pf.DiffType.NOD
-        rhs = config2_rhs(dev)
-        name = "config 2: 513x257x257 node-centred, EVEN/ODD x, PER y, UNB z, HEJ_4 (alpha 2)"
+        rhs = node513_rhs(dev)
+        name = "513x257x257 node-centred, EVEN/ODD x, PER y, UNB z, HEJ_4 (alpha 2)"
     else:
         n = 384
         nglob, lda, typ = [n] * 3, 3, 1
         bcs = [[[B.UNB] * 3, [B.UNB] * 3]] * 3
         h, L, center, kernel, odiff = [1 / n] * 3, [1.0] * 3, pf.CenterType.CELL_CENTER, "LGF_4", pf.DiffType.SPE
-        rhs = config3_rhs(n, dev)
-        name = "config 3: 384^3 cell, all UNB, LGF_4, ROT (spectral curl), 3-component vortex ring"
+        rhs = vortex_ring_rhs(n, dev)
+        name = "384^3 cell, all UNB, LGF_4, ROT (spectral curl), 3-component vortex ring"
     torch.cuda.synchronize()
     res = {}
     outs = {}
@@ -578,7 +578,7 @@ def main():
     if args.workload == "serve":
         run_serve(args)
         return
-    if args.workload in ("config2", "config3"):
+    if args.workload in ("node513", "rot384"):
         run_config(args)
         return
     if args.profile and args.grid:

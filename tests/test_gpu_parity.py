@@ -134,7 +134,7 @@ def test_rot_finite_difference_orders(odiff):
     assert rel_l2(g, o) <= TOL_FP64
 
 
-def config1_rhs(n=64):
+def gaussian_rhs(n=64):
     """Gaussian exp(-|x-c|^2/sigma^2), sigma = 0.1, c = (0.5,0.5,0.5), plus N(0, 1e-3) noise (seed 1)."""
     x = (np.arange(n) + 0.5) / n
     X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
@@ -143,11 +143,11 @@ def config1_rhs(n=64):
     return f[None]
 
 
-def test_config1_fp64_64cube_chat2():
+def test_gaussian_64cube_chat2_fp64():
     n = 64
     bcv = [[[4], [4]]] * 3
     h = [1.0 / n] * 3
-    rhs = config1_rhs(n)
+    rhs = gaussian_rhs(n)
     g = gpu_solve([n] * 3, 1, bcv, h, (1, 1, 1), CELL_CENTER, CHAT_2, rhs)
     o = oracle_solve([n] * 3, 1, bcv, h, (1, 1, 1), CELL_CENTER, CHAT_2, rhs)
     assert rel_l2(g, o) <= TOL_FP64
@@ -159,13 +159,13 @@ def test_fp32_mode_error(kernel):
     n = 64
     bcv = [[[4], [4]]] * 3
     h = [1.0 / n] * 3
-    rhs = config1_rhs(n)
+    rhs = gaussian_rhs(n)
     g = gpu_solve([n] * 3, 1, bcv, h, (1, 1, 1), CELL_CENTER, kernel, rhs, precision=32)
     o = oracle_solve([n] * 3, 1, bcv, h, (1, 1, 1), CELL_CENTER, kernel, rhs)
     assert rel_l2(g, o) <= 2e-6
 
 
-def test_config2_like_node_even_odd_per_unb_hej4():
+def test_node_even_odd_per_unb_hej4():
     """Node-centred, EVEN/ODD in x, PER in y, UNB in z, HEJ_4, isotropic h (33 x 17 x 17 nodes)."""
     nglob = [33, 17, 17]
     h = [1.0 / 16] * 3
