@@ -374,8 +374,9 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
         if (r >= NLD) {
             v[r] = mkc((T)0, (T)0);
         } else if constexpr (INS != SH_ANY) {
-            const C t = in[r * ls];
-            v[r] = valid ? t : mkc((T)0, (T)0);
+            // a lane past the last column reads the array's first element: its
+            // line (own exchange row, own Green's values) is never stored
+            v[r] = in[r * ls];
         } else {
             const bool ok = valid && p + F::P * r < a.nin;
             const C t = in[ok ? r * ls : 0];
