@@ -60,28 +60,6 @@ struct RowArgs {
     Prefetch pf;            // r2c / c2r rows
 };
 
-// x r2c rows + y forward columns (and the inverse pair) of the all-unbounded
-// x and y directions, one z plane per 16-CTA cluster (xy_cluster.cu).  FP32
-// working precision, user arrays FP64; x: LH user values per row (r2c of
-// length 2 LH), y: NY user rows (DFT of length 2 NY).
-struct XYArgs {
-    const void* in;          // forward: user array; backward: y spectrum (complex)
-    void* out;               // forward: y spectrum; backward: user array
-    void* nyq;               // x spectrum array at column LH (forward: written, backward: read)
-    int nz, ncomp;           // planes per component, components
-    int64_t u_s1, u_s2, u_cstr;   // user array (doubles): row y, plane z, component
-    int64_t s_l, s_o, s_c;        // y spectrum (complex): row ky, plane z, component
-    int64_t n_s1, n_s2, n_c;      // x spectrum (complex): row y, plane z, component
-    const void* tw_row;      // stage table of the LH-point DFT (first radix 32)
-    const void* tw_split;    // W_{2LH}^k, k < LH
-    const void* tw_col;      // stage table of the 2NY-point DFT (first radix 32)
-    int prefetch;            // L2 prefetch of the next plane's input
-};
-bool xy_cluster_supported(int LH, int NY);
-size_t xy_cluster_smem(int fwd, int LH, int NY);
-// a = nullptr: sets *nclusters (clusters the GPU co-schedules) and launches nothing
-cudaError_t launch_xy_cluster(int fwd, int LH, int NY, const XYArgs* a, int* nclusters, cudaStream_t s);
-
 // Fills `pf` for a 4-D view of 8-byte units (dims[0] fastest; strides in
 // bytes of dims 1..3) with box `box`; false (pf.nbox = 0) when the view does
 // not meet the tensor-map rules (16-byte aligned base and strides).

@@ -231,14 +231,6 @@ struct Solver {
     void do_fft_forward(const double* user_in, int nbatch);
     void fwd_pass(int ip, const double* user_in, int nbatch);
     void bwd_pass(int ip, double* user_out, int type, int nbatch);
-    flb::PassArgs fwd_args(int ip, const double* user_in, int nbatch);
-    flb::PassArgs bwd_args(int ip, double* user_out, int type, int nbatch);
-    // x and y passes of the all-unbounded FP32 pair as one 16-CTA cluster kernel
-    // per direction (xy_cluster.cu; flups_b200_set_xy_cluster)
-    bool xy_cluster = true;
-    mutable int xy_clusters[2] = {-1, -1};  // co-scheduled clusters (backward, forward); -1: not asked yet
-    bool xy_pair_ok(const flb::PassArgs& R, const flb::PassArgs& Cc, bool fwd) const;
-    void run_xy(flb::PassArgs R, flb::PassArgs Cc, bool fwd);
     // overlapped middle passes over x-slabs (flups_b200_set_overlap)
     bool overlap = false;
     // L2 prefetch of the next blocks' input in the row and column passes (flups_b200_set_prefetch)

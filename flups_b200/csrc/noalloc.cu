@@ -118,9 +118,6 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     void* keep[2] = {s->buf[0], s->buf[1]};
     s->buf[0] = wb[0];
     s->buf[1] = wb[1];
-    // separate x and y passes: the launches below cover the per-pass kernels only
-    const bool keep_xy = s->xy_cluster;
-    s->xy_cluster = false;
     s->dry = true;
     s->dry_passes.clear();
     s->dry_flags.clear();
@@ -137,7 +134,6 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     s->dry_fast.clear();
     s->buf[0] = keep[0];
     s->buf[1] = keep[1];
-    s->xy_cluster = keep_xy;
 
     // twiddle tables: one per distinct (length, layout)
     std::vector<TwSlot> slots;

@@ -1095,17 +1095,10 @@ static bool is_device_ptr(const void* p) {
 }
 
 void Solver::do_fft_forward(const double* user_in, int nbatch) {
-    if (ndim == 3) {
-        const PassArgs R = fwd_args(0, user_in, nbatch), Cc = fwd_args(1, user_in, nbatch);
-        if (xy_pair_ok(R, Cc, true)) {
-            run_xy(R, Cc, true);
-            return;
-        }
-    }
     for (int ip = 0; ip < ndim - 1; ++ip) fwd_pass(ip, user_in, nbatch);
 }
 
-PassArgs Solver::fwd_args(int ip, const double* user_in, int nbatch) {
+void Solver::fwd_pass(int ip, const double* user_in, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const DirPlan& p = fwd[ip];
@@ -1121,122 +1114,8 @@ PassArgs Solver::fwd_args(int ip, const double* user_in, int nbatch) {
     set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
     A.out = buf[ip % 2];
     fit_lines(A, es);
-    return A;
-}
-
-void Solver::fwd_pass(int ip, const double* user_in, int nbatch) {
-    const bool f64 = (precision == 64);
     static const char* fn[3] = {"fwd0", "fwd1", "fwd2"};
-    run_pass(fwd_args(ip, user_in, nbatch), f64, ip == 0 ? true : f64, f64, fn[ip]);
-}
-
-// The x r2c pass and the y forward pass (R, Cc as fwd_pass builds them), or
-// the y inverse and x c2r passes, as one cluster kernel: all-unbounded x and
-// y (both transforms zero-padded to twice the user size), FP32, the sizes
-// xy_cluster.cu is built for.  The spectrum column x = LH (one value per row)
-// goes through the x spectrum array and a one-column pass of the column kernel.
-bool Solver::xy_pair_ok(const PassArgs& R, const PassArgs& Cc, bool fwd) const {
-    if (!xy_cluster || !use_fast || precision != 32 || ndim != 3) return false;
-    if (R.axis != 0 || Cc.axis != 1 || R.fused || Cc.fused) return false;
-    if (fast_kind(R, false, fwd, !fwd) != 2 || fast_kind(Cc, false, false, false) != 1) return false;
-    const LineStage& SR = R.st[0];
-    const LineStage& SC = Cc.st[0];
-    const int LH = SR.M / 2, NY = SC.M / 2;
-    if (!xy_cluster_supported(LH, NY)) return false;
-    if (fwd) {
-        if (SR.spec[0].kind != LK_R2C || R.n_src != LH || SR.n_store != LH + 1) return false;
-        if (SC.spec[0].sign > 0 || Cc.n_src != NY || SC.n_store != 2 * NY) return false;
-    } else {
-        if (SR.spec[0].kind != LK_C2R || R.n_src != LH + 1 || SR.n_store != LH) return false;
-        if (SC.spec[0].sign < 0 || Cc.n_src != 2 * NY || SC.n_store != NY) return false;
-    }
-    // one row per (y, z) of the user array; x spectrum columns 0..LH
-    if (R.n_a != NY || Cc.n_a != LH + 1 || R.n_b != Cc.n_b || R.ncomp != Cc.ncomp) return false;
-    // 16-byte rows of doubles, 16-byte aligned y spectrum rows (L2 prefetch)
-    const int64_t* us = fwd ? R.in_str : R.out_str;
-    const int64_t ucs = fwd ? R.in_cstr : R.out_cstr;
-    if (us[1] % 2 || us[2] % 2 || ucs % 2) return false;
-    const int64_t* ys = fwd ? Cc.out_str : Cc.in_str;
-    if (ys[1] % 2 || ys[2] % 2) return false;
-    if (slab_dim >= 0 && slab_dim != 2) return false;
-    if (!dry) {
-        // 16 CTAs of about 210 KB of shared memory each must fit in one GPC
-        int& n = xy_clusters[fwd ? 1 : 0];
-        if (n < 0) {
-            int v = 0;
-            if (launch_xy_cluster(fwd ? 1 : 0, LH, NY, nullptr, &v, stream) != cudaSuccess) {
-                cudaGetLastError();
-                v = 0;
-            }
-            n = v;
-        }
-        if (n < 1) return false;
-    }
-    return true;
-}
-
-void Solver::run_xy(PassArgs R, PassArgs Cc, bool fwd) {
-    const int LH = R.st[0].M / 2, NY = Cc.st[0].M / 2;
-    // the one-column pass on the spectrum column x = LH (before the slab
-    // restriction: run_pass applies it)
-    PassArgs N = Cc;
-    N.in = (const char*)Cc.in + (size_t)LH * 8;
-    N.out = (char*)Cc.out + (size_t)LH * 8;
-    N.n_a = 1;
-    N.nlines = N.n_b;
-    if (slab_dim >= 0) {
-        restrict_slab(R, fwd, !fwd);
-        restrict_slab(Cc, false, false);
-    }
-    if (!fwd) run_pass(N, false, false, false, "bwd1n");
-    const double planes = (double)R.n_b * R.ncomp;
-    const double bytes = planes * ((double)LH * NY * 8.0 + (double)LH * 2 * NY * 8.0 + (double)NY * 8.0);
-    if (dry) {
-        dry_passes.push_back(R);
-        dry_flags.push_back(fwd ? 2 : 4);
-        dry_names.push_back(fwd ? "fwd01" : "bwd10");
-        dry_fast.push_back(5);
-    } else {
-        XYArgs x;
-        memset(&x, 0, sizeof(x));
-        x.nz = R.n_b;
-        x.ncomp = R.ncomp;
-        if (fwd) {
-            x.in = R.in;
-            x.out = Cc.out;
-            x.nyq = (char*)R.out + (size_t)LH * 8;
-            x.u_s1 = R.in_str[1];
-            x.u_s2 = R.in_str[2];
-            x.u_cstr = R.in_cstr;
-            x.s_l = Cc.out_str[1];
-            x.s_o = Cc.out_str[2];
-            x.s_c = Cc.out_cstr;
-            x.n_s1 = R.out_str[1];
-            x.n_s2 = R.out_str[2];
-            x.n_c = R.out_cstr;
-        } else {
-            x.in = Cc.in;
-            x.out = R.out;
-            x.nyq = (char*)const_cast<void*>(R.in) + (size_t)LH * 8;
-            x.u_s1 = R.out_str[1];
-            x.u_s2 = R.out_str[2];
-            x.u_cstr = R.out_cstr;
-            x.s_l = Cc.in_str[1];
-            x.s_o = Cc.in_str[2];
-            x.s_c = Cc.in_cstr;
-            x.n_s1 = R.in_str[1];
-            x.n_s2 = R.in_str[2];
-            x.n_c = R.in_cstr;
-        }
-        x.tw_row = stage_table(LH, false, 32);
-        x.tw_split = twiddle_plain(2 * LH, false);
-        x.tw_col = stage_table(2 * NY, false, 32);
-        x.prefetch = prefetch ? 1 : 0;
-        const int k = timed_begin(fwd ? "fwd01" : "bwd10", bytes);
-        check_cuda(launch_xy_cluster(fwd ? 1 : 0, LH, NY, &x, nullptr, stream), "x-y cluster launch");
-        timed_end(k);
-    }
-    if (fwd) run_pass(N, false, false, false, "fwd1n");
+    run_pass(A, f64, ip == 0 ? true : f64, f64, fn[ip]);
 }
 
 void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
@@ -1357,17 +1236,10 @@ void Solver::do_fused(int type, int nbatch) {
 }
 
 void Solver::do_backward(double* user_out, int type, int nbatch) {
-    if (ndim == 3) {
-        const PassArgs R = bwd_args(0, user_out, type, nbatch), Cc = bwd_args(1, user_out, type, nbatch);
-        if (xy_pair_ok(R, Cc, false)) {
-            run_xy(R, Cc, false);
-            return;
-        }
-    }
     for (int ip = ndim - 2; ip >= 0; --ip) bwd_pass(ip, user_out, type, nbatch);
 }
 
-PassArgs Solver::bwd_args(int ip, double* user_out, int type, int nbatch) {
+void Solver::bwd_pass(int ip, double* user_out, int type, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const DirPlan& p = (type == ROT) ? dif[ip] : bwd[ip];
@@ -1383,13 +1255,8 @@ PassArgs Solver::bwd_args(int ip, double* user_out, int type, int nbatch) {
         A.out = buf[(ip - 1) % 2];
     }
     fit_lines(A, es);
-    return A;
-}
-
-void Solver::bwd_pass(int ip, double* user_out, int type, int nbatch) {
-    const bool f64 = (precision == 64);
     static const char* bn[3] = {"bwd0", "bwd1", "bwd2"};
-    run_pass(bwd_args(ip, user_out, type, nbatch), f64, f64, ip == 0 ? true : f64, bn[ip]);
+    run_pass(A, f64, f64, ip == 0 ? true : f64, bn[ip]);
 }
 
 // Overlapped middle passes (STD, x transformed first, device arrays): after

@@ -116,7 +116,6 @@ def load_library(path=None):
         "flups_b200_set_col_tile": (None, [vp, c_int]),
         "flups_b200_set_overlap": (None, [vp, c_int]),
         "flups_b200_set_prefetch": (None, [vp, c_int]),
-        "flups_b200_set_xy_cluster": (None, [vp, c_int]),
         "flups_get_innerBuffer": (vp, [vp]),
         "flups_get_innerTopo_physical": (vp, [vp]),
         "flups_get_innerTopo_spectral": (vp, [vp]),
@@ -313,10 +312,6 @@ class Solver:
     def set_prefetch(self, on):
         """L2 prefetch of the next blocks' input in the row / column passes (default on)."""
         _lib.flups_b200_set_prefetch(self._solver, int(bool(on)))
-
-    def set_xy_cluster(self, on):
-        """x and y passes of the all-unbounded FP32 pair as one cluster kernel per direction (default on)."""
-        _lib.flups_b200_set_xy_cluster(self._solver, int(bool(on)))
 
     def set_col_tile(self, tile):
         """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""

@@ -95,13 +95,6 @@ void flups_b200_set_overlap(struct Solver* s, int on);
  * counterpart. */
 void flups_b200_set_prefetch(struct Solver* s, int on);
 
-/* x and y passes of the all-unbounded FP32 pair (x and y user sizes 256 or
- * 512, both zero-padded) as one 16-CTA cluster kernel per direction, the
- * plane's x spectrum kept in the cluster's shared memory (1 = on, the
- * default); 0 runs the separate x and y passes.  Same arithmetic either way
- * (results bitwise identical).  No reference counterpart. */
-void flups_b200_set_xy_cluster(struct Solver* s, int on);
-
 /* Force the CTA tile of every column pass: 0 = default or tuned, 1 = 256
  * threads, 2 = 128 threads.  For cross-checking the tiles. */
 void flups_b200_set_col_tile(struct Solver* s, int tile);
