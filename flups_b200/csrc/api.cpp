@@ -237,6 +237,30 @@ int flups_solve_graph(Solver* s, double* field, double* rhs, int nbatch, int typ
     return s->solve_graph(field, rhs, type, nbatch);
 }
 int flups_get_last_error(Solver* s) { return s->last_error; }
+
+int flups_b200_slab_info(Solver* s, int64_t info[7]) {
+    if (!s || !info) return -1;
+    const int e = s->slab_check(STD);
+    const ArrState& sp = s->st[s->ndim - 1];
+    info[0] = sp.n[0];
+    info[1] = sp.n[1];
+    info[2] = sp.n[2];
+    info[3] = s->row_pitch(sp);
+    info[4] = s->st[0].n[2];
+    info[5] = s->buf[(s->ndim - 2) % 2] ? 1 : 0;
+    info[6] = (s->precision == 64) ? 8 : 4;
+    return e;
+}
+void* flups_b200_slab_spectrum(Solver* s) {
+    if (!s || s->slab_check(STD) != 0) return nullptr;
+    s->ensure_buffers(1);
+    return s->buf[(s->ndim - 2) % 2];
+}
+int flups_b200_slab_forward(Solver* s, const double* rhs, int z0, int z1) { return s ? s->slab_forward(rhs, z0, z1) : -1; }
+int flups_b200_slab_fused(Solver* s, int x0, int x1, int type) { return s ? s->slab_fused(x0, x1, type) : -1; }
+int flups_b200_slab_backward(Solver* s, double* field, int z0, int z1, int type) {
+    return s ? s->slab_backward(field, z0, z1, type) : -1;
+}
 size_t flups_get_device_bytes(Solver* s, int nbatch) { return s->device_bytes(nbatch); }
 
 int flups_b200_plan_json(Solver* s, int type, int nbatch, char* out, int len) {

@@ -248,5 +248,13 @@ struct Solver {
     bool streamed_ok() const;
     void solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch);
     void restrict_slab(flb::PassArgs& A, bool in_f64, bool out_f64) const;
+    // one rank's steps of a z-slab decomposed solve (flups_b200_slab_*): the
+    // x and y passes of user planes [z0, z1), the last-direction pass of
+    // spectrum columns [x0, x1) over every plane, the inverse x and y passes
+    // of planes [z0, z1); the caller moves the spectrum between ranks
+    int slab_check(int type) const;
+    int slab_forward(const double* rhs, int z0, int z1);
+    int slab_fused(int x0, int x1, int type);
+    int slab_backward(double* field, int z0, int z1, int type);
     std::string plan_json(int type, int nbatch);
 };

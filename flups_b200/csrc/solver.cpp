@@ -1450,6 +1450,80 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
     else check_cuda(cudaGetLastError(), "solve");
 }
 
+// ---------------------------------------------------------------- z-slab decomposition
+// A solve split over ranks by planes of the last direction (the reference's
+// pencil solve with its transposes, Solver.cpp:629-715 / SwitchTopoX_a2a.cpp):
+// rank r owns user planes [z0, z1) and spectrum columns [x0, x1).  The x and
+// y passes of its planes and the inverse ones only touch those planes; the
+// last-direction pass needs every plane of its columns, so the spectrum is
+// exchanged (all-to-all) before and after it.  Each step is the single-GPU
+// pass restricted to a slab (slab_dim), so results equal the one-rank solve.
+// The user arrays of a step hold planes [z0, z1) only (scalar field, lda 1).
+int Solver::slab_check(int type) const {
+    if (!is_setup) return -1;
+    if (ndim != 3 || lda != 1 || type != STD) return -2;
+    if (fwd[0].dim != 0 || fwd[1].dim != 1 || fwd[2].dim != 2) return -2;
+    // the Green's spectrum is not folded along x, so a slab of columns reads its own part
+    if (gfold_M[0] != 0) return -2;
+    return 0;
+}
+
+// the user array of planes [z0, z1) seen as the full array (integer
+// arithmetic: that base may precede the allocation; the passes add the offset back)
+static uintptr_t slab_base(const void* p, int z0, int64_t plane_elems) {
+    return reinterpret_cast<uintptr_t>(p) - (uintptr_t)((int64_t)z0 * plane_elems * (int64_t)sizeof(double));
+}
+
+int Solver::slab_forward(const double* rhs, int z0, int z1) {
+    if (int e = slab_check(STD); e) return e;
+    if (!rhs || z0 < 0 || z1 > st[0].n[2] || z0 >= z1) return -2;
+    ensure_buffers(1);
+    int64_t ustr[3], ucstr;
+    set_strides_user(ustr, ucstr);
+    pass_idx = 0;
+    slab_dim = 2;
+    slab_lo = z0;
+    slab_hi = z1;
+    do_fft_forward(reinterpret_cast<const double*>(slab_base(rhs, z0, ustr[2])), 1);
+    slab_dim = -1;
+    collect_timing();
+    check_cuda(cudaGetLastError(), "slab forward");
+    return 0;
+}
+
+int Solver::slab_fused(int x0, int x1, int type) {
+    if (int e = slab_check(type); e) return e;
+    if (x0 < 0 || x1 > st[ndim - 1].n[0] || x0 >= x1) return -2;
+    ensure_buffers(1);
+    pass_idx = 0;
+    slab_dim = 0;
+    slab_lo = x0;
+    slab_hi = x1;
+    do_fused(type, 1);
+    slab_dim = -1;
+    collect_timing();
+    check_cuda(cudaGetLastError(), "slab fused pass");
+    return 0;
+}
+
+int Solver::slab_backward(double* field, int z0, int z1, int type) {
+    if (int e = slab_check(type); e) return e;
+    if (!field || z0 < 0 || z1 > st[0].n[2] || z0 >= z1) return -2;
+    ensure_buffers(1);
+    int64_t ustr[3], ucstr;
+    set_strides_user(ustr, ucstr);
+    pass_idx = 0;
+    slab_dim = 2;
+    slab_lo = z0;
+    slab_hi = z1;
+    do_backward(reinterpret_cast<double*>(slab_base(field, z0, ustr[2])), type, 1);
+    slab_dim = -1;
+    collect_timing();
+    if (!async) check_cuda(cudaStreamSynchronize(stream), "slab backward");
+    else check_cuda(cudaGetLastError(), "slab backward");
+    return 0;
+}
+
 // ---------------------------------------------------------------- advanced API
 // flups_get_innerBuffer / flups_get_innerTopo_* / flups_do_copy / do_FFT /
 // do_mult (Solver.cpp:518-530, 1281-1516).  The inner buffer is managed memory

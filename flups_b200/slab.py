@@ -1,0 +1,188 @@
+"""A solve split over ranks by planes of the last direction (z).
+
+The reference distributes a solve over MPI ranks as pencils and moves the
+data between the directions with all-to-all exchanges (Solver.cpp:629-715,
+SwitchTopoX_a2a.cpp:118-247).  Here every array stays x-fastest and the
+decomposition needs one transpose each way:
+
+  rank r owns user planes [z0, z1) and spectrum columns [x0, x1);
+  1. x and y forward passes of its planes           (flups_b200_slab_forward)
+  2. all-to-all: the block (its planes, columns of rank j) goes to rank j,
+     so rank r holds its columns over every plane
+  3. last-direction pass (forward DFT, Green's multiply, inverse DFT) of its
+     columns                                         (flups_b200_slab_fused)
+  4. all-to-all back: the block (planes of rank j, its columns) goes to rank j
+  5. y and x inverse passes of its planes           (flups_b200_slab_backward)
+
+Each step is the single-GPU pass restricted to a slab, so the result equals
+the one-rank solve bit for bit.  Every rank sets up a solver of the global
+problem (the Green's spectrum and the work arrays are global-sized); the
+user arrays of a rank hold its planes only.  Scalar fields (lda 1), STD
+solves, x, y and z transformed in that order.
+
+The exchanges take any transport with `alltoall(sends, recv_shapes)`:
+ProcessGroupTransport (torch.distributed: NCCL between GPUs, gloo on CPU),
+or the in-process exchange of `solve_local` (several ranks' solvers on one
+device).
+"""
+
+
+def split(n, parts, k):
+    """Balanced range [lo, hi) of part k of n items."""
+    return (k * n) // parts, ((k + 1) * n) // parts
+
+
+class SlabPlan:
+    """Planes and spectrum columns of every rank."""
+
+    def __init__(self, nz_user, nx_spec, world):
+        if world < 1 or world > nz_user or world > nx_spec:
+            raise ValueError(f"{world} ranks for {nz_user} planes and {nx_spec} spectrum columns")
+        self.world = world
+        self.z = [split(nz_user, world, k) for k in range(world)]
+        self.x = [split(nx_spec, world, k) for k in range(world)]
+
+
+# ---------------------------------------------------------------- exchanges
+# spec: the spectrum between the passes as a real tensor (nz, ny, pitch, 2)
+# (complex values as pairs); columns x < nx_spec are in use.
+
+def pack_forward(spec, plan, rank):
+    """Blocks (this rank's planes, columns of rank j) for every j."""
+    z0, z1 = plan.z[rank]
+    return [spec[z0:z1, :, a:b].contiguous() for a, b in plan.x]
+
+
+def unpack_forward(spec, plan, rank, recvs):
+    """recvs[i]: block (planes of rank i, this rank's columns) from rank i."""
+    a, b = plan.x[rank]
+    for i, (z0, z1) in enumerate(plan.z):
+        if i != rank:
+            spec[z0:z1, :, a:b].copy_(recvs[i].view(z1 - z0, spec.shape[1], b - a, spec.shape[3]))
+
+
+def pack_backward(spec, plan, rank):
+    """Blocks (planes of rank j, this rank's columns) for every j."""
+    a, b = plan.x[rank]
+    return [spec[z0:z1, :, a:b].contiguous() for z0, z1 in plan.z]
+
+
+def unpack_backward(spec, plan, rank, recvs):
+    """recvs[j]: block (this rank's planes, columns of rank j) from rank j."""
+    z0, z1 = plan.z[rank]
+    for j, (a, b) in enumerate(plan.x):
+        if j != rank:
+            spec[z0:z1, :, a:b].copy_(recvs[j].view(z1 - z0, spec.shape[1], b - a, spec.shape[3]))
+
+
+def recv_shapes_forward(spec, plan, rank):
+    a, b = plan.x[rank]
+    return [(z1 - z0, spec.shape[1], b - a, spec.shape[3]) for z0, z1 in plan.z]
+
+
+def recv_shapes_backward(spec, plan, rank):
+    z0, z1 = plan.z[rank]
+    return [(z1 - z0, spec.shape[1], b - a, spec.shape[3]) for a, b in plan.x]
+
+
+class ProcessGroupTransport:
+    """all-to-all through torch.distributed (one flat all_to_all_single)."""
+
+    def __init__(self, group=None):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.group = torch, dist, group
+
+    def alltoall(self, sends, recv_shapes):
+        torch = self.torch
+        send = torch.cat([s.reshape(-1) for s in sends])
+        sizes_in = [s.numel() for s in sends]
+        sizes_out = [a * b * c * d for a, b, c, d in recv_shapes]
+        recv = torch.empty(sum(sizes_out), dtype=send.dtype, device=send.device)
+        self.dist.all_to_all_single(recv, send, sizes_out, sizes_in, group=self.group)
+        return list(torch.split(recv, sizes_out))
+
+
+# ---------------------------------------------------------------- one rank
+
+class SlabRank:
+    """One rank's share of a z-slab decomposed solve on a set-up pyflups Solver."""
+
+    def __init__(self, solver, rank, world):
+        import torch
+        self.torch = torch
+        self.s, self.rank, self.world = solver, rank, world
+        code, (nx, ny, nz), pitch, nz_user, _, es = solver.slab_info()
+        if code != 0:
+            raise ValueError("this solver cannot run a z-slab solve (3-D, scalar, STD, directions x, y, z in order)")
+        self.plan = SlabPlan(nz_user, nx, world)
+        self.shape = (nz, ny, pitch, 2)
+        self.dtype = torch.float32 if es == 4 else torch.float64
+        self.z0, self.z1 = self.plan.z[rank]
+        self.x0, self.x1 = self.plan.x[rank]
+
+    def spectrum(self):
+        """The solver's spectrum work array as a device tensor (nz, ny, pitch, 2)."""
+        torch = self.torch
+        ptr = self.s.slab_spectrum_ptr()
+        if not ptr:
+            raise RuntimeError("no spectrum work array")
+        iface = {"shape": self.shape, "typestr": "<f4" if self.dtype == torch.float32 else "<f8",
+                 "data": (ptr, False), "version": 3}
+
+        class _View:
+            __cuda_array_interface__ = iface
+
+        return torch.as_tensor(_View(), device="cuda")
+
+    def _ok(self, code, what):
+        if code != 0:
+            raise RuntimeError(f"{what} failed with code {code} (last CUDA error {self.s.last_error()})")
+
+    def forward(self, rhs):
+        """rhs: this rank's planes of the right-hand side (device array, user layout)."""
+        self._ok(self.s.slab_forward(rhs, self.z0, self.z1), "slab forward")
+        self.s.synchronize()
+
+    def fused(self):
+        self._ok(self.s.slab_fused(self.x0, self.x1), "slab last-direction pass")
+        self.s.synchronize()
+
+    def backward(self, field):
+        """field: this rank's planes of the result (device array, user layout)."""
+        self._ok(self.s.slab_backward(field, self.z0, self.z1), "slab backward")
+        self.s.synchronize()
+
+    def solve(self, field, rhs, transport):
+        """The whole solve of this rank; every rank calls it with the same transport group."""
+        spec = self.spectrum()
+        self.forward(rhs)
+        recv = transport.alltoall(pack_forward(spec, self.plan, self.rank), recv_shapes_forward(spec, self.plan, self.rank))
+        unpack_forward(spec, self.plan, self.rank, recv)
+        self.torch.cuda.synchronize()
+        self.fused()
+        recv = transport.alltoall(pack_backward(spec, self.plan, self.rank), recv_shapes_backward(spec, self.plan, self.rank))
+        unpack_backward(spec, self.plan, self.rank, recv)
+        self.torch.cuda.synchronize()
+        self.backward(field)
+
+
+def solve_local(ranks, fields, rhss):
+    """The decomposed solve of several ranks' solvers in one process (one
+    device): the same steps, with the all-to-all done by device copies."""
+    torch = ranks[0].torch
+    specs = [r.spectrum() for r in ranks]
+    for r, rhs in zip(ranks, rhss):
+        r.forward(rhs)
+    sends = [pack_forward(sp, r.plan, r.rank) for r, sp in zip(ranks, specs)]
+    for r, sp in zip(ranks, specs):
+        unpack_forward(sp, r.plan, r.rank, [sends[i][r.rank] for i in range(len(ranks))])
+    torch.cuda.synchronize()
+    for r in ranks:
+        r.fused()
+    sends = [pack_backward(sp, r.plan, r.rank) for r, sp in zip(ranks, specs)]
+    for r, sp in zip(ranks, specs):
+        unpack_backward(sp, r.plan, r.rank, [sends[j][r.rank] for j in range(len(ranks))])
+    torch.cuda.synchronize()
+    for r, f in zip(ranks, fields):
+        r.backward(f)

@@ -7,6 +7,7 @@
 #define FLUPS_B200_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #include "flups_mpi.h"
 
@@ -98,6 +99,33 @@ void flups_b200_set_prefetch(struct Solver* s, int on);
 /* Force the CTA tile of every column pass: 0 = default or tuned, 1 = 256
  * threads, 2 = 128 threads.  For cross-checking the tiles. */
 void flups_b200_set_col_tile(struct Solver* s, int tile);
+
+/* One rank's steps of a solve split over ranks by planes of the last
+ * direction; replaces the reference's multi-rank pencil solve
+ * (src/Solver.cpp:629-715 with src/SwitchTopoX_a2a.cpp:118-247), whose
+ * transposes become two all-to-all exchanges of the spectrum that the
+ * caller does (flups_b200/slab.py: torch.distributed / NCCL).  Every rank
+ * sets up a solver of the global problem; rank r owns user planes [z0, z1)
+ * and spectrum columns [x0, x1).  Scalar fields, STD, directions x, y, z
+ * transformed in that order; otherwise the calls return -2 (-1: not set up).
+ *   flups_b200_slab_info: spectrum extents (info[0..2] = nx, ny, nz), row
+ *     pitch in complex values (info[3]), user planes (info[4]), work array
+ *     present (info[5]), bytes per real (info[6]); returns 0 when usable.
+ *   flups_b200_slab_spectrum: device address of the spectrum work array,
+ *     complex values at x + pitch (y + ny z).
+ *   flups_b200_slab_forward: x and y forward passes of planes [z0, z1);
+ *     rhs holds those planes only (device array, user layout).
+ *   flups_b200_slab_fused: last-direction pass (forward DFT, Green's
+ *     multiply, inverse DFT) of columns [x0, x1) over every plane.
+ *   flups_b200_slab_backward: y and x inverse passes of planes [z0, z1)
+ *     into field (those planes only).
+ * Each step is the single-rank pass restricted to a slab: the assembled
+ * field equals flups_solve's bit for bit. */
+int flups_b200_slab_info(struct Solver* s, int64_t info[7]);
+void* flups_b200_slab_spectrum(struct Solver* s);
+int flups_b200_slab_forward(struct Solver* s, const double* rhs, int z0, int z1);
+int flups_b200_slab_fused(struct Solver* s, int x0, int x1, int type);
+int flups_b200_slab_backward(struct Solver* s, double* field, int z0, int z1, int type);
 
 /* A solve (nbatch consecutive right-hand sides, as flups_solve_batch) of
  * device arrays replayed from a CUDA graph.  The first call for a given

@@ -1,0 +1,47 @@
+"""z-slab decomposed solve (flups_b200/slab.py) with 2 to 4 ranks' solvers
+in one process on one GPU (the all-to-all done by device copies): every step
+is the single-GPU pass on a slab, so the assembled field equals the one-rank
+solve bit for bit, FP32 and FP64.  The torch.distributed transport needs one
+GPU per rank; its exchange logic is covered on CPU (tests/test_slab_gloo.py)."""
+import numpy as np
+import pytest
+
+from gpu_helpers import make_solver, to_user
+from oracle.plans import CELL_CENTER, HEJ_2, LGF_2
+
+pytestmark = pytest.mark.gpu
+
+UNB = [[[4], [4]]] * 3
+
+
+@pytest.mark.parametrize("n,precision,world,kernel", [(64, 64, 2, HEJ_2), (128, 32, 3, LGF_2), (256, 32, 4, LGF_2),
+                                                      (96, 32, 2, HEJ_2)])
+def test_slab_solve_equals_one_rank(n, precision, world, kernel):
+    import torch
+    from flups_b200.slab import SlabRank, solve_local
+    rng = np.random.default_rng(n + world)
+    rhs = torch.from_numpy(to_user(rng.standard_normal((1, n, n, n)))).cuda()
+    t, s = make_solver([n] * 3, 1, UNB, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, kernel, precision=precision)
+    ref = torch.zeros_like(rhs)
+    s.solve(ref, rhs)
+    torch.cuda.synchronize()
+    assert s.last_error() == 0
+    keep = []
+    ranks = []
+    for r in range(world):
+        tr, sr = make_solver([n] * 3, 1, UNB, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, kernel, precision=precision)
+        keep.append((tr, sr))
+        ranks.append(SlabRank(sr, r, world))
+    rhs_parts = [rhs[0, r.z0:r.z1].contiguous() for r in ranks]
+    out_parts = [torch.full_like(p, float("nan")) for p in rhs_parts]
+    solve_local(ranks, out_parts, rhs_parts)
+    got = torch.cat(out_parts).unsqueeze(0)
+    assert all(sr.last_error() == 0 for _, sr in keep)
+    assert torch.equal(got, ref)
+
+
+def test_slab_refuses_other_problems():
+    from flups_b200.slab import SlabRank
+    t, s = make_solver([32] * 3, 3, [[[4] * 3, [4] * 3]] * 3, [1 / 32] * 3, [1.0] * 3, CELL_CENTER, HEJ_2)
+    with pytest.raises(ValueError):
+        SlabRank(s, 0, 2)
