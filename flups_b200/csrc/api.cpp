@@ -247,20 +247,16 @@ int flups_b200_slab_info(Solver* s, int64_t info[7]) {
     info[2] = sp.n[2];
     info[3] = s->row_pitch(sp);
     info[4] = s->st[0].n[2];
-    info[5] = s->buf[(s->ndim - 2) % 2] ? 1 : 0;
+    info[5] = s->xpitch;
     info[6] = (s->precision == 64) ? 8 : 4;
     return e;
 }
-void* flups_b200_slab_spectrum(Solver* s) {
-    if (!s || s->slab_check(STD) != 0) return nullptr;
-    s->ensure_buffers(1);
-    return s->buf[(s->ndim - 2) % 2];
-}
-int flups_b200_slab_forward(Solver* s, const double* rhs, int z0, int z1) { return s ? s->slab_forward(rhs, z0, z1) : -1; }
-int flups_b200_slab_fused(Solver* s, int x0, int x1, int type) { return s ? s->slab_fused(x0, x1, type) : -1; }
-int flups_b200_slab_backward(Solver* s, double* field, int z0, int z1, int type) {
-    return s ? s->slab_backward(field, z0, z1, type) : -1;
-}
+int flups_b200_slab_own(Solver* s, int z0, int z1, int x0, int x1) { return s ? s->slab_own(z0, z1, x0, x1) : -1; }
+void* flups_b200_slab_planes(Solver* s) { return (s && s->owned() && s->is_setup) ? s->buf[(s->ndim - 2) % 2] : nullptr; }
+void* flups_b200_slab_columns(Solver* s) { return (s && s->owned() && s->is_setup) ? s->xbuf : nullptr; }
+int flups_b200_slab_forward(Solver* s, const double* rhs) { return s ? s->slab_forward(rhs) : -1; }
+int flups_b200_slab_fused(Solver* s, int type) { return s ? s->slab_fused(type) : -1; }
+int flups_b200_slab_backward(Solver* s, double* field, int type) { return s ? s->slab_backward(field, type) : -1; }
 size_t flups_get_device_bytes(Solver* s, int nbatch) { return s->device_bytes(nbatch); }
 
 int flups_b200_plan_json(Solver* s, int type, int nbatch, char* out, int len) {

@@ -252,9 +252,18 @@ struct Solver {
     // x and y passes of user planes [z0, z1), the last-direction pass of
     // spectrum columns [x0, x1) over every plane, the inverse x and y passes
     // of planes [z0, z1); the caller moves the spectrum between ranks
+    // ownership set before setup (flups_b200_slab_own): planes [own[0], own[1])
+    // and spectrum columns [own[2], own[3]); the work arrays then hold those
+    // planes only, and `xbuf` (pitch `xpitch`) holds the columns over every plane
+    int own[4] = {-1, -1, -1, -1};
+    void* xbuf = nullptr;
+    int64_t xpitch = 0;
+    bool owned() const { return own[0] >= 0; }
+    int slab_own(int z0, int z1, int x0, int x1);
+    void* work_base(int b) const;
     int slab_check(int type) const;
-    int slab_forward(const double* rhs, int z0, int z1);
-    int slab_fused(int x0, int x1, int type);
-    int slab_backward(double* field, int z0, int z1, int type);
+    int slab_forward(const double* rhs);
+    int slab_fused(int type);
+    int slab_backward(double* field, int type);
     std::string plan_json(int type, int nbatch);
 };

@@ -77,6 +77,7 @@ int fail(int code, const char* msg) {
 extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int type) {
     if (!s) return fail(-1, "solver is NULL");
     if (!s->is_setup) return fail(-1, "flups_setup must be called first (it computes the Green's spectrum)");
+    if (s->owned()) return fail(-2, "this solver holds one rank's share of the planes (flups_b200_slab_own)");
     if (!field || !rhs) return fail(-2, "field and rhs must not be NULL");
     if (type == ROT && (s->lda != 3 || s->odiff == NOD)) return fail(-2, "ROT needs lda = 3 and a derivative order");
     for (const void* p : {(const void*)field, (const void*)rhs}) {

@@ -173,6 +173,7 @@ Solver::~Solver() {
     }
     for (auto& b : buf)
         if (b) cudaFree(b);
+    if (xbuf) cudaFree(xbuf);
     if (green) cudaFree(green);
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
@@ -1048,11 +1049,20 @@ void Solver::setup() {
 void Solver::ensure_buffers(int nbatch) {
     const bool f64 = (precision == 64);
     const size_t es = f64 ? 8 : 4;
+    if (owned()) {
+        // one rank's share: the planes it owns, and its spectrum columns over every plane
+        FLB_CHECK(nbatch == 1, "a solver set up for a share of the planes solves one field at a time");
+        const ArrState& sp = st[ndim - 1];
+        const size_t xneed = (size_t)xpitch * sp.n[1] * sp.n[2] * 2;
+        if (!xbuf) check_cuda(cudaMalloc(&xbuf, xneed * es), "column work buffer");
+    }
     for (int b = 0; b < 2; ++b) {
         size_t need = 0;
         for (int k = 1; k < ndim; ++k) {
             if ((k - 1) % 2 != b) continue;
-            need = std::max(need, state_reals(k, nbatch));
+            size_t r = state_reals(k, nbatch);
+            if (owned()) r = r / (size_t)st[k].n[2] * (size_t)(own[1] - own[0]);
+            need = std::max(need, r);
         }
         if (need > buf_elems[b]) {
             drop_graphs();  // captured solves point at the old arrays
@@ -1109,10 +1119,10 @@ void Solver::fwd_pass(int ip, const double* user_in, int nbatch) {
         A.in = user_in;
     } else {
         set_strides_internal(A.in_str, A.in_cstr, st[ip]);
-        A.in = buf[(ip - 1) % 2];
+        A.in = work_base((ip - 1) % 2);
     }
     set_strides_internal(A.out_str, A.out_cstr, st[ip + 1]);
-    A.out = buf[ip % 2];
+    A.out = work_base(ip % 2);
     fit_lines(A, es);
     static const char* fn[3] = {"fwd0", "fwd1", "fwd2"};
     run_pass(A, f64, ip == 0 ? true : f64, f64, fn[ip]);
@@ -1220,6 +1230,17 @@ void Solver::do_fused(int type, int nbatch) {
         set_strides_internal(A.out_str, A.out_cstr, st[ipl]);
         A.in = buf[(ipl - 1) % 2];
         A.out = buf[(ipl - 1) % 2];
+        if (owned()) {
+            // the rank's columns over every plane, column own[2] first (the
+            // slab restriction along x adds own[2] columns back)
+            const ArrState& sp = st[ipl];
+            const int64_t str[3] = {1, xpitch, xpitch * sp.n[1]};
+            for (int d = 0; d < 3; ++d) A.in_str[d] = A.out_str[d] = str[d];
+            A.in_cstr = A.out_cstr = xpitch * sp.n[1] * sp.n[2];
+            const uintptr_t base = reinterpret_cast<uintptr_t>(xbuf) - (uintptr_t)own[2] * (uintptr_t)(2 * es);
+            A.in = reinterpret_cast<const void*>(base);
+            A.out = reinterpret_cast<void*>(base);
+        }
         fit_lines(A, es);
         if (rot && nbatch > 1) {
             const int64_t per = A.in_cstr * 3 * (st[ipl].cplx ? 2 : 1);
@@ -1246,13 +1267,13 @@ void Solver::bwd_pass(int ip, double* user_out, int type, int nbatch) {
     PassArgs A = base_pass(fwd[ip].dim, st[ip + 1], lda * nbatch, lda);
     A.st[0] = stage_backward(p, fwd[ip], ip, f64);
     set_strides_internal(A.in_str, A.in_cstr, st[ip + 1]);
-    A.in = buf[ip % 2];
+    A.in = work_base(ip % 2);
     if (ip == 0) {
         set_strides_user(A.out_str, A.out_cstr);
         A.out = user_out;
     } else {
         set_strides_internal(A.out_str, A.out_cstr, st[ip]);
-        A.out = buf[(ip - 1) % 2];
+        A.out = work_base((ip - 1) % 2);
     }
     fit_lines(A, es);
     static const char* bn[3] = {"bwd0", "bwd1", "bwd2"};
@@ -1318,6 +1339,7 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     FLB_CHECK(field != nullptr, "field is NULL");
     FLB_CHECK(rhs != nullptr, "rhs is NULL");
     FLB_CHECK(nbatch >= 1, "nbatch must be >= 1");
+    FLB_CHECK(!owned(), "this solver holds one rank's share of the planes: use the flups_b200_slab_* steps");
     ensure_buffers(nbatch);
     if (autotune) autotune_passes(type, nbatch);
     const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
@@ -1458,9 +1480,12 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
 // last-direction pass needs every plane of its columns, so the spectrum is
 // exchanged (all-to-all) before and after it.  Each step is the single-GPU
 // pass restricted to a slab (slab_dim), so results equal the one-rank solve.
-// The user arrays of a step hold planes [z0, z1) only (scalar field, lda 1).
+// The work arrays hold the rank's planes only (`work_base` places them where
+// the full array would start, so the passes' slab offsets land on them) and
+// `xbuf` holds its columns over every plane: a rank's memory falls with the
+// rank count, apart from the Green's spectrum, which every rank keeps.  The
+// user arrays of a step hold the rank's planes only (scalar field, lda 1).
 int Solver::slab_check(int type) const {
-    if (!is_setup) return -1;
     if (ndim != 3 || lda != 1 || type != STD) return -2;
     if (fwd[0].dim != 0 || fwd[1].dim != 1 || fwd[2].dim != 2) return -2;
     // the Green's spectrum is not folded along x, so a slab of columns reads its own part
@@ -1468,37 +1493,56 @@ int Solver::slab_check(int type) const {
     return 0;
 }
 
-// the user array of planes [z0, z1) seen as the full array (integer
-// arithmetic: that base may precede the allocation; the passes add the offset back)
+int Solver::slab_own(int z0, int z1, int x0, int x1) {
+    if (is_setup || owned()) return -1;
+    if (int e = slab_check(STD); e) return e;
+    if (z0 < 0 || z1 > st[0].n[2] || z0 >= z1 || x0 < 0 || x1 > st[ndim - 1].n[0] || x0 >= x1) return -2;
+    own[0] = z0;
+    own[1] = z1;
+    own[2] = x0;
+    own[3] = x1;
+    const int64_t q = (precision == 64) ? 8 : 16;  // complex values per 128 bytes
+    xpitch = (x1 - x0 + q - 1) / q * q;
+    return 0;
+}
+
+// the array of buffer b seen from plane 0 (integer arithmetic: that base may
+// precede the allocation; a pass restricted to the owned planes adds them back)
+void* Solver::work_base(int b) const {
+    if (!owned() || !buf[b]) return buf[b];
+    const int k = b + 1;  // 3-D: buffer 0 holds state 1, buffer 1 state 2
+    const int64_t plane = row_pitch(st[k]) * st[k].n[1] * (st[k].cplx ? 2 : 1) * (precision == 64 ? 8 : 4);
+    return reinterpret_cast<void*>(reinterpret_cast<uintptr_t>(buf[b]) - (uintptr_t)((int64_t)own[0] * plane));
+}
+
+// the user array of the owned planes seen from plane 0 (integer arithmetic, as above)
 static uintptr_t slab_base(const void* p, int z0, int64_t plane_elems) {
     return reinterpret_cast<uintptr_t>(p) - (uintptr_t)((int64_t)z0 * plane_elems * (int64_t)sizeof(double));
 }
 
-int Solver::slab_forward(const double* rhs, int z0, int z1) {
-    if (int e = slab_check(STD); e) return e;
-    if (!rhs || z0 < 0 || z1 > st[0].n[2] || z0 >= z1) return -2;
-    ensure_buffers(1);
+int Solver::slab_forward(const double* rhs) {
+    if (!is_setup || !owned()) return -1;
+    if (!rhs) return -2;
     int64_t ustr[3], ucstr;
     set_strides_user(ustr, ucstr);
     pass_idx = 0;
     slab_dim = 2;
-    slab_lo = z0;
-    slab_hi = z1;
-    do_fft_forward(reinterpret_cast<const double*>(slab_base(rhs, z0, ustr[2])), 1);
+    slab_lo = own[0];
+    slab_hi = own[1];
+    do_fft_forward(reinterpret_cast<const double*>(slab_base(rhs, own[0], ustr[2])), 1);
     slab_dim = -1;
     collect_timing();
     check_cuda(cudaGetLastError(), "slab forward");
     return 0;
 }
 
-int Solver::slab_fused(int x0, int x1, int type) {
+int Solver::slab_fused(int type) {
+    if (!is_setup || !owned()) return -1;
     if (int e = slab_check(type); e) return e;
-    if (x0 < 0 || x1 > st[ndim - 1].n[0] || x0 >= x1) return -2;
-    ensure_buffers(1);
     pass_idx = 0;
     slab_dim = 0;
-    slab_lo = x0;
-    slab_hi = x1;
+    slab_lo = own[2];
+    slab_hi = own[3];
     do_fused(type, 1);
     slab_dim = -1;
     collect_timing();
@@ -1506,17 +1550,17 @@ int Solver::slab_fused(int x0, int x1, int type) {
     return 0;
 }
 
-int Solver::slab_backward(double* field, int z0, int z1, int type) {
+int Solver::slab_backward(double* field, int type) {
+    if (!is_setup || !owned()) return -1;
     if (int e = slab_check(type); e) return e;
-    if (!field || z0 < 0 || z1 > st[0].n[2] || z0 >= z1) return -2;
-    ensure_buffers(1);
+    if (!field) return -2;
     int64_t ustr[3], ucstr;
     set_strides_user(ustr, ucstr);
     pass_idx = 0;
     slab_dim = 2;
-    slab_lo = z0;
-    slab_hi = z1;
-    do_backward(reinterpret_cast<double*>(slab_base(field, z0, ustr[2])), type, 1);
+    slab_lo = own[0];
+    slab_hi = own[1];
+    do_backward(reinterpret_cast<double*>(slab_base(field, own[0], ustr[2])), type, 1);
     slab_dim = -1;
     collect_timing();
     if (!async) check_cuda(cudaStreamSynchronize(stream), "slab backward");
@@ -1585,6 +1629,7 @@ void Solver::adv_copy(const Topology* topo, double* data, int sign) {
 
 void Solver::adv_fft(double* data, int sign) {
     FLB_CHECK(data != nullptr, "data is NULL");
+    FLB_CHECK(!owned(), "this solver holds one rank's share of the planes: use the flups_b200_slab_* steps");
     FLB_CHECK(sign == FLUPS_FORWARD || sign == FLUPS_BACKWARD || sign == FLUPS_BACKWARD_DIFF, "unknown sign %d", sign);
     FLB_CHECK(sign != FLUPS_BACKWARD_DIFF || have_diff, "FLUPS_BACKWARD_DIFF needs a solver set up with a derivative order");
     ensure_inner();
@@ -1729,7 +1774,7 @@ void Solver::autotune_passes(int type, int nbatch) {
 // (field, rhs, nbatch, type) runs a plain solve (which allocates and tunes what
 // it needs), then captures a second one; later calls only launch the graph.
 int Solver::solve_graph(double* field, double* rhs, int type, int nbatch) {
-    if (!is_setup || !field || !rhs || nbatch < 1) return -1;
+    if (!is_setup || !field || !rhs || nbatch < 1 || owned()) return -1;
     if (!is_device_ptr(field) || !is_device_ptr(rhs)) return -2;
     GraphKey k{field, rhs, nbatch, type};
     auto it = graphs.find(k);

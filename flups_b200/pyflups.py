@@ -117,10 +117,12 @@ def load_library(path=None):
         "flups_b200_set_overlap": (None, [vp, c_int]),
         "flups_b200_set_prefetch": (None, [vp, c_int]),
         "flups_b200_slab_info": (c_int, [vp, POINTER(ctypes.c_int64)]),
-        "flups_b200_slab_spectrum": (vp, [vp]),
-        "flups_b200_slab_forward": (c_int, [vp, vp, c_int, c_int]),
-        "flups_b200_slab_fused": (c_int, [vp, c_int, c_int, c_int]),
-        "flups_b200_slab_backward": (c_int, [vp, vp, c_int, c_int, c_int]),
+        "flups_b200_slab_own": (c_int, [vp, c_int, c_int, c_int, c_int]),
+        "flups_b200_slab_planes": (vp, [vp]),
+        "flups_b200_slab_columns": (vp, [vp]),
+        "flups_b200_slab_forward": (c_int, [vp, vp]),
+        "flups_b200_slab_fused": (c_int, [vp, c_int]),
+        "flups_b200_slab_backward": (c_int, [vp, vp, c_int]),
         "flups_get_innerBuffer": (vp, [vp]),
         "flups_get_innerTopo_physical": (vp, [vp]),
         "flups_get_innerTopo_spectral": (vp, [vp]),
@@ -318,26 +320,32 @@ class Solver:
         """L2 prefetch of the next blocks' input in the row / column passes (default on)."""
         _lib.flups_b200_set_prefetch(self._solver, int(bool(on)))
 
-    # ---- one rank's steps of a z-slab decomposed solve (flups_b200/slab.py drives them)
+    # ---- one rank's share of a z-slab decomposed solve (flups_b200/slab.py drives it)
     def slab_info(self):
-        """(code, spectrum extents (nx, ny, nz), row pitch, user planes, work array present, element bytes);
-        code 0 when the solver can run the slab steps."""
+        """(code, spectrum extents (nx, ny, nz), plane-array row pitch, user planes, column-array row pitch,
+        bytes per real); code 0 when the problem qualifies."""
         info = (ctypes.c_int64 * 7)()
         code = _lib.flups_b200_slab_info(self._solver, info)
-        return code, (info[0], info[1], info[2]), info[3], info[4], bool(info[5]), info[6]
+        return code, (info[0], info[1], info[2]), info[3], info[4], info[5], info[6]
 
-    def slab_spectrum_ptr(self):
-        """Device address of the work array that holds the spectrum between the slab steps."""
-        return _lib.flups_b200_slab_spectrum(self._solver)
+    def slab_own(self, z0, z1, x0, x1):
+        """Before setup: the planes [z0, z1) and spectrum columns [x0, x1) this solver owns."""
+        return _lib.flups_b200_slab_own(self._solver, int(z0), int(z1), int(x0), int(x1))
 
-    def slab_forward(self, rhs, z0, z1):
-        return _lib.flups_b200_slab_forward(self._solver, _ptr(rhs), int(z0), int(z1))
+    def slab_planes_ptr(self):
+        return _lib.flups_b200_slab_planes(self._solver)
 
-    def slab_fused(self, x0, x1, solver_type=SolverType.STD):
-        return _lib.flups_b200_slab_fused(self._solver, int(x0), int(x1), int(solver_type))
+    def slab_columns_ptr(self):
+        return _lib.flups_b200_slab_columns(self._solver)
 
-    def slab_backward(self, field, z0, z1, solver_type=SolverType.STD):
-        return _lib.flups_b200_slab_backward(self._solver, _ptr(field), int(z0), int(z1), int(solver_type))
+    def slab_forward(self, rhs):
+        return _lib.flups_b200_slab_forward(self._solver, _ptr(rhs))
+
+    def slab_fused(self, solver_type=SolverType.STD):
+        return _lib.flups_b200_slab_fused(self._solver, int(solver_type))
+
+    def slab_backward(self, field, solver_type=SolverType.STD):
+        return _lib.flups_b200_slab_backward(self._solver, _ptr(field), int(solver_type))
 
     def set_col_tile(self, tile):
         """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""

@@ -15,10 +15,11 @@ decomposition needs one transpose each way:
   5. y and x inverse passes of its planes           (flups_b200_slab_backward)
 
 Each step is the single-GPU pass restricted to a slab, so the result equals
-the one-rank solve bit for bit.  Every rank sets up a solver of the global
-problem (the Green's spectrum and the work arrays are global-sized); the
-user arrays of a rank hold its planes only.  Scalar fields (lda 1), STD
-solves, x, y and z transformed in that order.
+the one-rank solve bit for bit.  A rank's solver holds its planes (the plane
+array) and its columns over every plane (the column array), so its work
+memory falls with the rank count; every rank keeps the global Green's
+spectrum.  The user arrays of a rank hold its planes only.  Scalar fields
+(lda 1), STD solves, x, y and z transformed in that order.
 
 The exchanges take any transport with `alltoall(sends, recv_shapes)`:
 ProcessGroupTransport (torch.distributed: NCCL between GPUs, gloo on CPU),
@@ -44,45 +45,43 @@ class SlabPlan:
 
 
 # ---------------------------------------------------------------- exchanges
-# spec: the spectrum between the passes as a real tensor (nz, ny, pitch, 2)
-# (complex values as pairs); columns x < nx_spec are in use.
+# planes: this rank's plane array (nz_r, ny, pitch, 2) (complex values as
+# pairs), columns: its column array (nz, ny, cpitch, 2); spectrum columns
+# x < nx_spec are in use.
 
-def pack_forward(spec, plan, rank):
+def pack_forward(planes, plan, rank):
     """Blocks (this rank's planes, columns of rank j) for every j."""
-    z0, z1 = plan.z[rank]
-    return [spec[z0:z1, :, a:b].contiguous() for a, b in plan.x]
+    return [planes[:, :, a:b].contiguous() for a, b in plan.x]
 
 
-def unpack_forward(spec, plan, rank, recvs):
+def unpack_forward(columns, plan, rank, recvs):
     """recvs[i]: block (planes of rank i, this rank's columns) from rank i."""
     a, b = plan.x[rank]
     for i, (z0, z1) in enumerate(plan.z):
-        if i != rank:
-            spec[z0:z1, :, a:b].copy_(recvs[i].view(z1 - z0, spec.shape[1], b - a, spec.shape[3]))
+        columns[z0:z1, :, :b - a].copy_(recvs[i].view(z1 - z0, columns.shape[1], b - a, columns.shape[3]))
 
 
-def pack_backward(spec, plan, rank):
+def pack_backward(columns, plan, rank):
     """Blocks (planes of rank j, this rank's columns) for every j."""
     a, b = plan.x[rank]
-    return [spec[z0:z1, :, a:b].contiguous() for z0, z1 in plan.z]
+    return [columns[z0:z1, :, :b - a].contiguous() for z0, z1 in plan.z]
 
 
-def unpack_backward(spec, plan, rank, recvs):
+def unpack_backward(planes, plan, rank, recvs):
     """recvs[j]: block (this rank's planes, columns of rank j) from rank j."""
     z0, z1 = plan.z[rank]
     for j, (a, b) in enumerate(plan.x):
-        if j != rank:
-            spec[z0:z1, :, a:b].copy_(recvs[j].view(z1 - z0, spec.shape[1], b - a, spec.shape[3]))
+        planes[:, :, a:b].copy_(recvs[j].view(z1 - z0, planes.shape[1], b - a, planes.shape[3]))
 
 
-def recv_shapes_forward(spec, plan, rank):
+def recv_shapes_forward(columns, plan, rank):
     a, b = plan.x[rank]
-    return [(z1 - z0, spec.shape[1], b - a, spec.shape[3]) for z0, z1 in plan.z]
+    return [(z1 - z0, columns.shape[1], b - a, columns.shape[3]) for z0, z1 in plan.z]
 
 
-def recv_shapes_backward(spec, plan, rank):
+def recv_shapes_backward(planes, plan, rank):
     z0, z1 = plan.z[rank]
-    return [(z1 - z0, spec.shape[1], b - a, spec.shape[3]) for a, b in plan.x]
+    return [(z1 - z0, planes.shape[1], b - a, planes.shape[3]) for a, b in plan.x]
 
 
 class ProcessGroupTransport:
@@ -106,7 +105,9 @@ class ProcessGroupTransport:
 # ---------------------------------------------------------------- one rank
 
 class SlabRank:
-    """One rank's share of a z-slab decomposed solve on a set-up pyflups Solver."""
+    """One rank's share of a z-slab decomposed solve: takes a pyflups Solver
+    that is initialised (green type, precision set) but not set up, gives it
+    its planes and columns and sets it up."""
 
     def __init__(self, solver, rank, world):
         import torch
@@ -116,18 +117,20 @@ class SlabRank:
         if code != 0:
             raise ValueError("this solver cannot run a z-slab solve (3-D, scalar, STD, directions x, y, z in order)")
         self.plan = SlabPlan(nz_user, nx, world)
-        self.shape = (nz, ny, pitch, 2)
-        self.dtype = torch.float32 if es == 4 else torch.float64
         self.z0, self.z1 = self.plan.z[rank]
         self.x0, self.x1 = self.plan.x[rank]
+        self._ok(solver.slab_own(self.z0, self.z1, self.x0, self.x1), "slab_own")
+        solver.setup()
+        code, _, _, _, cpitch, _ = solver.slab_info()
+        self.dtype = torch.float32 if es == 4 else torch.float64
+        self.planes_shape = (self.z1 - self.z0, ny, pitch, 2)
+        self.columns_shape = (nz, ny, cpitch, 2)
 
-    def spectrum(self):
-        """The solver's spectrum work array as a device tensor (nz, ny, pitch, 2)."""
+    def _view(self, ptr, shape):
         torch = self.torch
-        ptr = self.s.slab_spectrum_ptr()
         if not ptr:
-            raise RuntimeError("no spectrum work array")
-        iface = {"shape": self.shape, "typestr": "<f4" if self.dtype == torch.float32 else "<f8",
+            raise RuntimeError("no work array (set up?)")
+        iface = {"shape": shape, "typestr": "<f4" if self.dtype == torch.float32 else "<f8",
                  "data": (ptr, False), "version": 3}
 
         class _View:
@@ -135,34 +138,44 @@ class SlabRank:
 
         return torch.as_tensor(_View(), device="cuda")
 
+    def planes(self):
+        """The plane array (owned planes of the spectrum between the passes) as a device tensor."""
+        return self._view(self.s.slab_planes_ptr(), self.planes_shape)
+
+    def columns(self):
+        """The column array (owned columns over every plane) as a device tensor."""
+        return self._view(self.s.slab_columns_ptr(), self.columns_shape)
+
     def _ok(self, code, what):
         if code != 0:
             raise RuntimeError(f"{what} failed with code {code} (last CUDA error {self.s.last_error()})")
 
     def forward(self, rhs):
         """rhs: this rank's planes of the right-hand side (device array, user layout)."""
-        self._ok(self.s.slab_forward(rhs, self.z0, self.z1), "slab forward")
+        self._ok(self.s.slab_forward(rhs), "slab forward")
         self.s.synchronize()
 
     def fused(self):
-        self._ok(self.s.slab_fused(self.x0, self.x1), "slab last-direction pass")
+        self._ok(self.s.slab_fused(), "slab last-direction pass")
         self.s.synchronize()
 
     def backward(self, field):
         """field: this rank's planes of the result (device array, user layout)."""
-        self._ok(self.s.slab_backward(field, self.z0, self.z1), "slab backward")
+        self._ok(self.s.slab_backward(field), "slab backward")
         self.s.synchronize()
 
     def solve(self, field, rhs, transport):
         """The whole solve of this rank; every rank calls it with the same transport group."""
-        spec = self.spectrum()
+        planes, columns = self.planes(), self.columns()
         self.forward(rhs)
-        recv = transport.alltoall(pack_forward(spec, self.plan, self.rank), recv_shapes_forward(spec, self.plan, self.rank))
-        unpack_forward(spec, self.plan, self.rank, recv)
+        recv = transport.alltoall(pack_forward(planes, self.plan, self.rank),
+                                  recv_shapes_forward(columns, self.plan, self.rank))
+        unpack_forward(columns, self.plan, self.rank, recv)
         self.torch.cuda.synchronize()
         self.fused()
-        recv = transport.alltoall(pack_backward(spec, self.plan, self.rank), recv_shapes_backward(spec, self.plan, self.rank))
-        unpack_backward(spec, self.plan, self.rank, recv)
+        recv = transport.alltoall(pack_backward(columns, self.plan, self.rank),
+                                  recv_shapes_backward(planes, self.plan, self.rank))
+        unpack_backward(planes, self.plan, self.rank, recv)
         self.torch.cuda.synchronize()
         self.backward(field)
 
@@ -171,18 +184,19 @@ def solve_local(ranks, fields, rhss):
     """The decomposed solve of several ranks' solvers in one process (one
     device): the same steps, with the all-to-all done by device copies."""
     torch = ranks[0].torch
-    specs = [r.spectrum() for r in ranks]
+    planes = [r.planes() for r in ranks]
+    columns = [r.columns() for r in ranks]
     for r, rhs in zip(ranks, rhss):
         r.forward(rhs)
-    sends = [pack_forward(sp, r.plan, r.rank) for r, sp in zip(ranks, specs)]
-    for r, sp in zip(ranks, specs):
-        unpack_forward(sp, r.plan, r.rank, [sends[i][r.rank] for i in range(len(ranks))])
+    sends = [pack_forward(p, r.plan, r.rank) for r, p in zip(ranks, planes)]
+    for r, c in zip(ranks, columns):
+        unpack_forward(c, r.plan, r.rank, [sends[i][r.rank] for i in range(len(ranks))])
     torch.cuda.synchronize()
     for r in ranks:
         r.fused()
-    sends = [pack_backward(sp, r.plan, r.rank) for r, sp in zip(ranks, specs)]
-    for r, sp in zip(ranks, specs):
-        unpack_backward(sp, r.plan, r.rank, [sends[j][r.rank] for j in range(len(ranks))])
+    sends = [pack_backward(c, r.plan, r.rank) for r, c in zip(ranks, columns)]
+    for r, p in zip(ranks, planes):
+        unpack_backward(p, r.plan, r.rank, [sends[j][r.rank] for j in range(len(ranks))])
     torch.cuda.synchronize()
     for r, f in zip(ranks, fields):
         r.backward(f)

@@ -100,32 +100,44 @@ void flups_b200_set_prefetch(struct Solver* s, int on);
  * threads, 2 = 128 threads.  For cross-checking the tiles. */
 void flups_b200_set_col_tile(struct Solver* s, int tile);
 
-/* One rank's steps of a solve split over ranks by planes of the last
+/* One rank's share of a solve split over ranks by planes of the last
  * direction; replaces the reference's multi-rank pencil solve
  * (src/Solver.cpp:629-715 with src/SwitchTopoX_a2a.cpp:118-247), whose
  * transposes become two all-to-all exchanges of the spectrum that the
- * caller does (flups_b200/slab.py: torch.distributed / NCCL).  Every rank
- * sets up a solver of the global problem; rank r owns user planes [z0, z1)
- * and spectrum columns [x0, x1).  Scalar fields, STD, directions x, y, z
- * transformed in that order; otherwise the calls return -2 (-1: not set up).
+ * caller does (flups_b200/slab.py: torch.distributed / NCCL).  Rank r owns
+ * user planes [z0, z1) and spectrum columns [x0, x1); scalar fields, STD,
+ * directions x, y, z transformed in that order (else -2; -1: wrong order of
+ * calls).  Every rank keeps the global Green's spectrum; its work arrays
+ * hold its planes and its columns only.
  *   flups_b200_slab_info: spectrum extents (info[0..2] = nx, ny, nz), row
- *     pitch in complex values (info[3]), user planes (info[4]), work array
- *     present (info[5]), bytes per real (info[6]); returns 0 when usable.
- *   flups_b200_slab_spectrum: device address of the spectrum work array,
- *     complex values at x + pitch (y + ny z).
- *   flups_b200_slab_forward: x and y forward passes of planes [z0, z1);
- *     rhs holds those planes only (device array, user layout).
+ *     pitch of the plane array in complex values (info[3]), user planes
+ *     (info[4]), row pitch of the column array (info[5], after slab_own),
+ *     bytes per real (info[6]); returns 0 when the problem qualifies.
+ *   flups_b200_slab_own: before flups_setup, the planes and columns this
+ *     solver owns (flups_solve and the advanced calls then refuse it).
+ *   flups_b200_slab_planes: device array of the owned planes of the spectrum
+ *     between the passes, complex value (x, y, z - z0) at
+ *     x + pitch (y + ny (z - z0)).
+ *   flups_b200_slab_columns: device array of the owned columns over every
+ *     plane, complex value (x - x0, y, z) at (x - x0) + cpitch (y + ny z).
+ *   flups_b200_slab_forward: x and y forward passes of the owned planes of
+ *     rhs (device array holding those planes only, user layout) into the
+ *     plane array.
  *   flups_b200_slab_fused: last-direction pass (forward DFT, Green's
- *     multiply, inverse DFT) of columns [x0, x1) over every plane.
- *   flups_b200_slab_backward: y and x inverse passes of planes [z0, z1)
- *     into field (those planes only).
- * Each step is the single-rank pass restricted to a slab: the assembled
- * field equals flups_solve's bit for bit. */
+ *     multiply, inverse DFT) of the column array, in place.
+ *   flups_b200_slab_backward: y and x inverse passes of the plane array into
+ *     field (the owned planes only).
+ * Between forward and fused the caller moves block (owned planes, columns of
+ * rank j) of every rank's plane array into rank j's column array, and back
+ * between fused and backward.  Each step is the single-rank pass restricted
+ * to a slab: the assembled field equals flups_solve's bit for bit. */
 int flups_b200_slab_info(struct Solver* s, int64_t info[7]);
-void* flups_b200_slab_spectrum(struct Solver* s);
-int flups_b200_slab_forward(struct Solver* s, const double* rhs, int z0, int z1);
-int flups_b200_slab_fused(struct Solver* s, int x0, int x1, int type);
-int flups_b200_slab_backward(struct Solver* s, double* field, int z0, int z1, int type);
+int flups_b200_slab_own(struct Solver* s, int z0, int z1, int x0, int x1);
+void* flups_b200_slab_planes(struct Solver* s);
+void* flups_b200_slab_columns(struct Solver* s);
+int flups_b200_slab_forward(struct Solver* s, const double* rhs);
+int flups_b200_slab_fused(struct Solver* s, int type);
+int flups_b200_slab_backward(struct Solver* s, double* field, int type);
 
 /* A solve (nbatch consecutive right-hand sides, as flups_solve_batch) of
  * device arrays replayed from a CUDA graph.  The first call for a given

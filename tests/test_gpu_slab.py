@@ -1,8 +1,9 @@
 """z-slab decomposed solve (flups_b200/slab.py) with 2 to 4 ranks' solvers
 in one process on one GPU (the all-to-all done by device copies): every step
-is the single-GPU pass on a slab, so the assembled field equals the one-rank
-solve bit for bit, FP32 and FP64.  The torch.distributed transport needs one
-GPU per rank; its exchange logic is covered on CPU (tests/test_slab_gloo.py)."""
+is the single-GPU pass on a slab of a rank's own arrays, so the assembled
+field equals the one-rank solve bit for bit, FP32 and FP64.  The
+torch.distributed transport needs one GPU per rank; its exchange logic is
+covered on CPU (tests/test_slab_gloo.py)."""
 import numpy as np
 import pytest
 
@@ -12,6 +13,18 @@ from oracle.plans import CELL_CENTER, HEJ_2, LGF_2
 pytestmark = pytest.mark.gpu
 
 UNB = [[[4], [4]]] * 3
+
+
+def _unset_solver(n, kernel, precision):
+    from flups_b200 import pyflups as pf
+    t = pf.Topology(0, 1, [n] * 3)
+    s = pf.Solver(t, [[pf.BoundaryType.UNB, pf.BoundaryType.UNB]] * 3, [1.0 / n] * 3, [1.0] * 3,
+                  center_type=[CELL_CENTER] * 3)
+    s.set_green_type(kernel)
+    s.set_alpha(2.0)
+    if precision != 64:
+        s.set_precision(precision)
+    return t, s
 
 
 @pytest.mark.parametrize("n,precision,world,kernel", [(64, 64, 2, HEJ_2), (128, 32, 3, LGF_2), (256, 32, 4, LGF_2),
@@ -26,10 +39,10 @@ def test_slab_solve_equals_one_rank(n, precision, world, kernel):
     s.solve(ref, rhs)
     torch.cuda.synchronize()
     assert s.last_error() == 0
-    keep = []
-    ranks = []
+    full = s.device_bytes(1)
+    keep, ranks = [], []
     for r in range(world):
-        tr, sr = make_solver([n] * 3, 1, UNB, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, kernel, precision=precision)
+        tr, sr = _unset_solver(n, kernel, precision)
         keep.append((tr, sr))
         ranks.append(SlabRank(sr, r, world))
     rhs_parts = [rhs[0, r.z0:r.z1].contiguous() for r in ranks]
@@ -38,10 +51,17 @@ def test_slab_solve_equals_one_rank(n, precision, world, kernel):
     got = torch.cat(out_parts).unsqueeze(0)
     assert all(sr.last_error() == 0 for _, sr in keep)
     assert torch.equal(got, ref)
+    # a rank's plane and column arrays hold about 1/world of the work arrays
+    esz = 8 if precision == 64 else 4
+    for r in ranks:
+        work = (np.prod(r.planes_shape) + np.prod(r.columns_shape)) * esz
+        assert work < 1.6 * full / world
 
 
 def test_slab_refuses_other_problems():
+    from flups_b200 import pyflups as pf
     from flups_b200.slab import SlabRank
-    t, s = make_solver([32] * 3, 3, [[[4] * 3, [4] * 3]] * 3, [1 / 32] * 3, [1.0] * 3, CELL_CENTER, HEJ_2)
+    t = pf.Topology(0, 3, [32] * 3)
+    s = pf.Solver(t, [[pf.BoundaryType.UNB, pf.BoundaryType.UNB]] * 3, [1 / 32] * 3, [1.0] * 3)
     with pytest.raises(ValueError):
         SlabRank(s, 0, 2)

@@ -1,6 +1,8 @@
 """Exchange steps of the z-slab decomposed solve (flups_b200/slab.py) across
 processes on CPU: gloo, world_size 2 and 3, with spectra whose values encode
-(plane, row, column, part), so every moved block is checked in place."""
+(plane, row, column, part), so every moved block is checked in place: the
+forward exchange from plane arrays into column arrays, the backward one
+from column arrays into plane arrays."""
 import os
 import socket
 import sys
@@ -44,17 +46,19 @@ def _worker(rank, world, port, q):
         code = _code(torch)
         z0, z1 = plan.z[rank]
         x0, x1 = plan.x[rank]
-        # after the forward passes a rank has valid values in its planes only
-        spec = torch.full(SHAPE, -1.0, dtype=torch.float64)
-        spec[z0:z1] = code[z0:z1]
-        recv = t.alltoall(pack_forward(spec, plan, rank), recv_shapes_forward(spec, plan, rank))
-        unpack_forward(spec, plan, rank, recv)
-        ok_fwd = bool(torch.equal(spec[:, :, x0:x1], code[:, :, x0:x1]))
+        cp = (x1 - x0 + 3) // 4 * 4
+        # after the forward passes a rank's plane array holds its planes
+        planes = code[z0:z1].clone()
+        columns = torch.full((SHAPE[0], SHAPE[1], cp, SHAPE[3]), -1.0, dtype=torch.float64)
+        recv = t.alltoall(pack_forward(planes, plan, rank), recv_shapes_forward(columns, plan, rank))
+        unpack_forward(columns, plan, rank, recv)
+        ok_fwd = bool(torch.equal(columns[:, :, :x1 - x0], code[:, :, x0:x1]))
         # the last-direction pass changes this rank's columns over every plane
-        spec[:, :, x0:x1] = -code[:, :, x0:x1]
-        recv = t.alltoall(pack_backward(spec, plan, rank), recv_shapes_backward(spec, plan, rank))
-        unpack_backward(spec, plan, rank, recv)
-        ok_bwd = bool(torch.equal(spec[z0:z1, :, :NX], -code[z0:z1, :, :NX]))
+        columns[:, :, :x1 - x0] = -code[:, :, x0:x1]
+        planes.fill_(0.0)
+        recv = t.alltoall(pack_backward(columns, plan, rank), recv_shapes_backward(planes, plan, rank))
+        unpack_backward(planes, plan, rank, recv)
+        ok_bwd = bool(torch.equal(planes[:, :, :NX], -code[z0:z1, :, :NX]))
         q.put((rank, ok_fwd, ok_bwd))
     finally:
         dist.destroy_process_group()
