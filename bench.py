@@ -19,8 +19,9 @@ Reported (one JSON line on rank 0):
 
 --impl reference times the reference's CPU algorithm (the oracle port: the
 reference needs FFTW, MPI and h3lpr, which this image does not have) on the
-same metric.  --gpus N runs N independent replicas (one per GPU): the solve
-does not shard.
+same metric.  --gpus N runs N independent replicas (one per GPU, weak
+scaling).  --workload slab instead splits one solve over the ranks by z
+planes (flups_b200/slab.py: NCCL all-to-all of the spectrum; strong scaling).
 """
 import argparse
 import json
@@ -50,7 +51,7 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "node513", "rot384"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "node513", "rot384", "slab"],
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
@@ -538,6 +539,78 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def run_slab(args):
+    """One n^3 all-unbounded LGF_2 FP32 solve split over the ranks by z planes
+    (flups_b200/slab.py): the x and y passes of a rank's planes, an NCCL
+    all-to-all of the spectrum, the last-direction pass of its columns, the
+    all-to-all back and the inverse passes.  Strong scaling: the same solve
+    at every rank count; device arrays (a rank holds its planes of rhs and
+    field); the step time is the slowest rank's."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+    from flups_b200 import pyflups as pf
+    from flups_b200.slab import ProcessGroupTransport, SlabRank
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if "MASTER_ADDR" not in os.environ:
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0", WORLD_SIZE="1")
+        sk.close()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    try:
+        n = args.n
+        B = pf.BoundaryType
+        t = pf.Topology(0, 1, [n, n, n])
+        s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1.0 / n] * 3, [1.0] * 3)
+        s.set_green_type(pf.GreenType[args.kernel])
+        s.set_precision(32)
+        r = SlabRank(s, rank, world)
+        rhs = rhs_gaussians(n, device=dev)[r.z0:r.z1].contiguous()
+        field = torch.empty_like(rhs)
+        tr = ProcessGroupTransport()
+        for _ in range(max(3, args.warmup)):
+            r.solve(field, rhs, tr)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as cs:
+            e0.record()
+            for _ in range(args.steps):
+                r.solve(field, rhs, tr)
+            e1.record()
+            torch.cuda.synchronize()
+        dist.barrier()
+        tt = torch.tensor([e0.elapsed_time(e1) / args.steps], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": n ** 3 / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sum of 8 Gaussians)",
+                "config": {"workload": f"{n}^3 cell-centred all-unbounded scalar Poisson, {args.kernel}, FP32, "
+                                       f"split over {world} rank(s) by z planes", "grid": [n, n, n],
+                           "parallelism": f"z-slab x{world}",
+                           "l2_flush": "inputs larger than L2 at n = 512"},
+                "e2e": {"value": None, "note": "device arrays only: the slab steps take each rank's planes on its GPU"},
+                "gpu_launches": 5 * args.steps,
+                "work_bytes_per_rank": int((np.prod(r.planes_shape) + np.prod(r.columns_shape)) * 4),
+                "clocks": cs.summary(),
+            }
+            print(json.dumps(line), flush=True)
+        del r, s, t
+    finally:
+        dist.destroy_process_group()
+
+
 def run_profile_grid(args):
     """FP32 solves of a seeded random right-hand side on an anisotropic all-unbounded
     grid (cell-centred, h = 1/NX), for ncu captures; prints the mean solve time."""
@@ -580,6 +653,9 @@ def main():
         return
     if args.workload in ("node513", "rot384"):
         run_config(args)
+        return
+    if args.workload == "slab":
+        run_slab(args)
         return
     if args.profile and args.grid:
         run_profile_grid(args)

@@ -49,9 +49,23 @@ class SlabPlan:
 # pairs), columns: its column array (nz, ny, cpitch, 2); spectrum columns
 # x < nx_spec are in use.
 
-def pack_forward(planes, plan, rank):
+def _pack(blocks, out):
+    """The blocks as new contiguous tensors, or copied into consecutive
+    segments of the flat tensor `out` (one copy, no concatenation after)."""
+    if out is None:
+        return [b.contiguous() for b in blocks]
+    views, off = [], 0
+    for b in blocks:
+        v = out[off:off + b.numel()].view(b.shape)
+        v.copy_(b)
+        views.append(v)
+        off += b.numel()
+    return views
+
+
+def pack_forward(planes, plan, rank, out=None):
     """Blocks (this rank's planes, columns of rank j) for every j."""
-    return [planes[:, :, a:b].contiguous() for a, b in plan.x]
+    return _pack([planes[:, :, a:b] for a, b in plan.x], out)
 
 
 def unpack_forward(columns, plan, rank, recvs):
@@ -61,10 +75,10 @@ def unpack_forward(columns, plan, rank, recvs):
         columns[z0:z1, :, :b - a].copy_(recvs[i].view(z1 - z0, columns.shape[1], b - a, columns.shape[3]))
 
 
-def pack_backward(columns, plan, rank):
+def pack_backward(columns, plan, rank, out=None):
     """Blocks (planes of rank j, this rank's columns) for every j."""
     a, b = plan.x[rank]
-    return [columns[z0:z1, :, :b - a].contiguous() for z0, z1 in plan.z]
+    return _pack([columns[z0:z1, :, :b - a] for z0, z1 in plan.z], out)
 
 
 def unpack_backward(planes, plan, rank, recvs):
@@ -92,13 +106,17 @@ class ProcessGroupTransport:
         import torch.distributed as dist
         self.torch, self.dist, self.group = torch, dist, group
 
-    def alltoall(self, sends, recv_shapes):
+    def alltoall(self, sends, recv_shapes, send_flat=None, recv_flat=None):
+        """sends: the blocks for every rank (consecutive views of `send_flat`
+        when it is given, else concatenated here); returns the received
+        blocks (views of `recv_flat` when it is given)."""
         torch = self.torch
-        send = torch.cat([s.reshape(-1) for s in sends])
+        send = send_flat if send_flat is not None else torch.cat([s.reshape(-1) for s in sends])
         sizes_in = [s.numel() for s in sends]
         sizes_out = [a * b * c * d for a, b, c, d in recv_shapes]
-        recv = torch.empty(sum(sizes_out), dtype=send.dtype, device=send.device)
-        self.dist.all_to_all_single(recv, send, sizes_out, sizes_in, group=self.group)
+        recv = recv_flat[:sum(sizes_out)] if recv_flat is not None else \
+            torch.empty(sum(sizes_out), dtype=send.dtype, device=send.device)
+        self.dist.all_to_all_single(recv, send[:sum(sizes_in)], sizes_out, sizes_in, group=self.group)
         return list(torch.split(recv, sizes_out))
 
 
@@ -166,17 +184,27 @@ class SlabRank:
 
     def solve(self, field, rhs, transport):
         """The whole solve of this rank; every rank calls it with the same transport group."""
+        torch = self.torch
         planes, columns = self.planes(), self.columns()
+        if getattr(self, "_flat", None) is None:
+            # exchange buffers, kept: the largest block set a rank sends or receives
+            nx = self.plan.x[-1][1]
+            ny = self.planes_shape[1]
+            own = (self.z1 - self.z0) * ny * nx * 2
+            cols = self.columns_shape[0] * ny * (self.x1 - self.x0) * 2
+            self._flat = (torch.empty(max(own, cols), dtype=self.dtype, device=planes.device),
+                          torch.empty(max(own, cols), dtype=self.dtype, device=planes.device))
+        sbuf, rbuf = self._flat
         self.forward(rhs)
-        recv = transport.alltoall(pack_forward(planes, self.plan, self.rank),
-                                  recv_shapes_forward(columns, self.plan, self.rank))
+        recv = transport.alltoall(pack_forward(planes, self.plan, self.rank, sbuf),
+                                  recv_shapes_forward(columns, self.plan, self.rank), sbuf, rbuf)
         unpack_forward(columns, self.plan, self.rank, recv)
-        self.torch.cuda.synchronize()
+        torch.cuda.synchronize()
         self.fused()
-        recv = transport.alltoall(pack_backward(columns, self.plan, self.rank),
-                                  recv_shapes_backward(planes, self.plan, self.rank))
+        recv = transport.alltoall(pack_backward(columns, self.plan, self.rank, sbuf),
+                                  recv_shapes_backward(planes, self.plan, self.rank), sbuf, rbuf)
         unpack_backward(planes, self.plan, self.rank, recv)
-        self.torch.cuda.synchronize()
+        torch.cuda.synchronize()
         self.backward(field)
 
 

@@ -59,6 +59,19 @@ def _worker(rank, world, port, q):
         recv = t.alltoall(pack_backward(columns, plan, rank), recv_shapes_backward(planes, plan, rank))
         unpack_backward(planes, plan, rank, recv)
         ok_bwd = bool(torch.equal(planes[:, :, :NX], -code[z0:z1, :, :NX]))
+        # the same exchanges through reusable flat send / receive buffers
+        sbuf = torch.empty(4096, dtype=torch.float64)
+        rbuf = torch.empty(4096, dtype=torch.float64)
+        planes = code[z0:z1].clone()
+        columns.fill_(-1.0)
+        recv = t.alltoall(pack_forward(planes, plan, rank, sbuf), recv_shapes_forward(columns, plan, rank), sbuf, rbuf)
+        unpack_forward(columns, plan, rank, recv)
+        ok_fwd = ok_fwd and bool(torch.equal(columns[:, :, :x1 - x0], code[:, :, x0:x1]))
+        columns[:, :, :x1 - x0] = -code[:, :, x0:x1]
+        planes.fill_(0.0)
+        recv = t.alltoall(pack_backward(columns, plan, rank, sbuf), recv_shapes_backward(planes, plan, rank), sbuf, rbuf)
+        unpack_backward(planes, plan, rank, recv)
+        ok_bwd = ok_bwd and bool(torch.equal(planes[:, :, :NX], -code[z0:z1, :, :NX]))
         q.put((rank, ok_fwd, ok_bwd))
     finally:
         dist.destroy_process_group()
