@@ -260,6 +260,8 @@ struct Solver {
     int64_t xpitch = 0;
     bool owned() const { return own[0] >= 0; }
     int slab_own(int z0, int z1, int x0, int x1);
+    void* green_share = nullptr;  // allocation of a share's columns of the Green's spectrum
+    void slice_green();
     void* work_base(int b) const;
     int slab_check(int type) const;
     int slab_forward(const double* rhs);

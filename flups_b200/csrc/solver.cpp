@@ -174,7 +174,8 @@ Solver::~Solver() {
     for (auto& b : buf)
         if (b) cudaFree(b);
     if (xbuf) cudaFree(xbuf);
-    if (green) cudaFree(green);
+    if (green_share) cudaFree(green_share);
+    else if (green) cudaFree(green);
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
     if (stage_out) cudaFree(stage_out);
@@ -1042,8 +1043,32 @@ void Solver::setup() {
     FLB_CHECK(e == cudaSuccess && ndev > 0, "no CUDA device available (%s): this library has no CPU path",
               cudaGetErrorString(e));
     compute_green();
+    if (owned()) slice_green();
     ensure_buffers(1);
     is_setup = true;
+}
+
+// A solver set up for a share keeps only its columns [own[2], own[3]) of the
+// folded Green's spectrum (x is not folded there), rows on 128-byte
+// boundaries; `green` is placed where the full array would start, so the
+// x-slab offset of the last-direction pass lands on the share.
+void Solver::slice_green() {
+    const bool f64 = (precision == 64);
+    const size_t es = f64 ? 8 : 4;
+    FLB_CHECK(gfold_M[0] == 0 && gstr[0] == 1 && own[3] <= gfold_n[0] && gstr[2] == gstr[1] * gfold_n[1],
+              "the Green's spectrum cannot be split by columns");
+    const int64_t gq = f64 ? 16 : 32;
+    const int64_t w = own[3] - own[2], wp = (w + gq - 1) / gq * gq;
+    void* gc = nullptr;
+    check_cuda(cudaMalloc(&gc, (size_t)wp * gfold_n[1] * gfold_n[2] * es), "Green spectrum share");
+    check_cuda(cudaMemcpy2D(gc, wp * es, (const char*)green + own[2] * es, gstr[1] * es, w * es,
+                            (size_t)gfold_n[1] * gfold_n[2], cudaMemcpyDeviceToDevice),
+               "Green spectrum share copy");
+    cudaFree(green);
+    green_share = gc;
+    green = reinterpret_cast<void*>(reinterpret_cast<uintptr_t>(gc) - (uintptr_t)own[2] * es);
+    gstr[1] = wp;
+    gstr[2] = wp * gfold_n[1];
 }
 
 void Solver::ensure_buffers(int nbatch) {
@@ -1087,10 +1112,14 @@ size_t Solver::device_bytes(int nbatch) const {
         size_t need = 0;
         for (int k = 1; k < ndim; ++k) {
             if ((k - 1) % 2 != b) continue;
-            need = std::max(need, state_reals(k, nbatch));
+            size_t r = state_reals(k, nbatch);
+            if (owned()) r = r / (size_t)st[k].n[2] * (size_t)(own[1] - own[0]);
+            need = std::max(need, r);
         }
         total += need * es;
     }
+    if (owned()) total += (size_t)xpitch * st[ndim - 1].n[1] * st[ndim - 1].n[2] * 2 * es;
+    // (a share holds its columns of the Green's spectrum: gstr describes that array after set-up)
     total += (size_t)gstr[2] * gfold_n[2] * es;
     return total;
 }
@@ -1483,7 +1512,7 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
 // The work arrays hold the rank's planes only (`work_base` places them where
 // the full array would start, so the passes' slab offsets land on them) and
 // `xbuf` holds its columns over every plane: a rank's memory falls with the
-// rank count, apart from the Green's spectrum, which every rank keeps.  The
+// rank count; the Green's spectrum is cut to its columns at set-up.  The
 // user arrays of a step hold the rank's planes only (scalar field, lda 1).
 int Solver::slab_check(int type) const {
     if (ndim != 3 || lda != 1 || type != STD) return -2;

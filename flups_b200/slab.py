@@ -16,9 +16,8 @@ decomposition needs one transpose each way:
 
 Each step is the single-GPU pass restricted to a slab, so the result equals
 the one-rank solve bit for bit.  A rank's solver holds its planes (the plane
-array) and its columns over every plane (the column array), so its work
-memory falls with the rank count; every rank keeps the global Green's
-spectrum.  The user arrays of a rank hold its planes only.  Scalar fields
+array), its columns over every plane (the column array) and its columns of
+the Green's spectrum, so its device memory falls with the rank count.  The user arrays of a rank hold its planes only.  Scalar fields
 (lda 1), STD solves, x, y and z transformed in that order.
 
 The exchanges take any transport with `alltoall(sends, recv_shapes)`:

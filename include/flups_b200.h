@@ -107,8 +107,8 @@ void flups_b200_set_col_tile(struct Solver* s, int tile);
  * caller does (flups_b200/slab.py: torch.distributed / NCCL).  Rank r owns
  * user planes [z0, z1) and spectrum columns [x0, x1); scalar fields, STD,
  * directions x, y, z transformed in that order (else -2; -1: wrong order of
- * calls).  Every rank keeps the global Green's spectrum; its work arrays
- * hold its planes and its columns only.
+ * calls).  A rank's work arrays hold its planes and its columns only, and
+ * set-up keeps only its columns of the Green's spectrum.
  *   flups_b200_slab_info: spectrum extents (info[0..2] = nx, ny, nz), row
  *     pitch of the plane array in complex values (info[3]), user planes
  *     (info[4]), row pitch of the column array (info[5], after slab_own),

@@ -51,11 +51,10 @@ def test_slab_solve_equals_one_rank(n, precision, world, kernel):
     got = torch.cat(out_parts).unsqueeze(0)
     assert all(sr.last_error() == 0 for _, sr in keep)
     assert torch.equal(got, ref)
-    # a rank's plane and column arrays hold about 1/world of the work arrays
-    esz = 8 if precision == 64 else 4
+    # a rank's arrays (planes, columns, its columns of the Green's spectrum)
+    # are about 1/world of the one-rank solver's, plus row padding
     for r in ranks:
-        work = (np.prod(r.planes_shape) + np.prod(r.columns_shape)) * esz
-        assert work < 1.6 * full / world
+        assert r.s.device_bytes(1) < full * (1.0 / world + 0.45)
 
 
 def test_slab_refuses_other_problems():
