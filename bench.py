@@ -55,6 +55,9 @@ def parse():
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
+    ap.add_argument("--slab-exchange", default="peer", choices=["peer", "alltoall"],
+                    help="slab: y passes that store into / load from every rank's column array over CUDA IPC "
+                         "(peer; NCCL all-to-all if any rank cannot open the others' arrays), or NCCL all-to-all")
     ap.add_argument("--overlap", type=int, default=0, help="1: overlap the per-x-slab middle passes on three streams")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="with --profile: an all-unbounded grid NX x NY x NZ instead of n^3 (for ncu captures of one pass "
@@ -552,7 +555,7 @@ def run_slab(args):
     import torch
     import torch.distributed as dist
     from flups_b200 import pyflups as pf
-    from flups_b200.slab import ProcessGroupTransport, SlabRank
+    from flups_b200.slab import ProcessGroupTransport, SlabRank, connect_peers, solve_connected
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -575,8 +578,27 @@ def run_slab(args):
         rhs = rhs_gaussians(n, device=dev)[r.z0:r.z1].contiguous()
         field = torch.empty_like(rhs)
         tr = ProcessGroupTransport()
+        peer = args.slab_exchange == "peer"
+        if peer:
+            ok = 1
+            try:
+                connect_peers(r)
+            except RuntimeError:
+                ok = 0
+            flag = torch.tensor([ok], device=dev)
+            dist.all_reduce(flag, op=dist.ReduceOp.MIN)
+            peer = bool(flag.item())
+            if not peer:
+                r.s.slab_peers([], [], [])
+
+        def step():
+            if peer:
+                solve_connected(r, field, rhs)
+            else:
+                r.solve(field, rhs, tr)
+
         for _ in range(max(3, args.warmup)):
-            r.solve(field, rhs, tr)
+            step()
         torch.cuda.synchronize()
         dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -584,7 +606,7 @@ def run_slab(args):
         with ClockSampler(local) as cs:
             e0.record()
             for _ in range(args.steps):
-                r.solve(field, rhs, tr)
+                step()
             e1.record()
             torch.cuda.synchronize()
         dist.barrier()
@@ -599,6 +621,8 @@ def run_slab(args):
                 "config": {"workload": f"{n}^3 cell-centred all-unbounded scalar Poisson, {args.kernel}, FP32, "
                                        f"split over {world} rank(s) by z planes", "grid": [n, n, n],
                            "parallelism": f"z-slab x{world}",
+                           "exchange": ("y passes store into / load from the owners' column arrays (CUDA IPC, NVLink)"
+                                        if peer else "NCCL all_to_all_single of packed blocks"),
                            "l2_flush": "inputs larger than L2 at n = 512"},
                 "e2e": {"value": None, "note": "device arrays only: the slab steps take each rank's planes on its GPU"},
                 "gpu_launches": 5 * args.steps,
@@ -606,6 +630,12 @@ def run_slab(args):
                 "clocks": cs.summary(),
             }
             print(json.dumps(line), flush=True)
+        if peer:
+            r.s.slab_peers([], [], [])
+            from flups_b200 import pyflups as _pf
+            for ptr in getattr(r, "_opened", []):
+                _pf.load_library().flups_b200_ipc_close(ptr)
+        dist.barrier()
         del r, s, t
     finally:
         dist.destroy_process_group()

@@ -257,6 +257,30 @@ void* flups_b200_slab_columns(Solver* s) { return (s && s->owned() && s->is_setu
 int flups_b200_slab_forward(Solver* s, const double* rhs) { return s ? s->slab_forward(rhs) : -1; }
 int flups_b200_slab_fused(Solver* s, int type) { return s ? s->slab_fused(type) : -1; }
 int flups_b200_slab_backward(Solver* s, double* field, int type) { return s ? s->slab_backward(field, type) : -1; }
+int flups_b200_slab_peers(Solver* s, int n, void* const* cols, const int* xs, const int64_t* pitch) {
+    return s ? s->slab_peers(n, cols, xs, pitch) : -1;
+}
+int flups_b200_ipc_handle(const void* dev_ptr, void* handle) {
+    if (!dev_ptr || !handle) return -2;
+    cudaIpcMemHandle_t h;
+    if (cudaIpcGetMemHandle(&h, const_cast<void*>(dev_ptr)) != cudaSuccess) {
+        cudaGetLastError();
+        return -4;
+    }
+    memcpy(handle, &h, sizeof(h));
+    return 0;
+}
+int flups_b200_ipc_open(const void* handle, void** dev_ptr) {
+    if (!handle || !dev_ptr) return -2;
+    cudaIpcMemHandle_t h;
+    memcpy(&h, handle, sizeof(h));
+    if (cudaIpcOpenMemHandle(dev_ptr, h, cudaIpcMemLazyEnablePeerAccess) != cudaSuccess) {
+        cudaGetLastError();
+        return -4;
+    }
+    return 0;
+}
+int flups_b200_ipc_close(void* dev_ptr) { return cudaIpcCloseMemHandle(dev_ptr) == cudaSuccess ? 0 : -4; }
 size_t flups_get_device_bytes(Solver* s, int nbatch) { return s->device_bytes(nbatch); }
 
 int flups_b200_plan_json(Solver* s, int type, int nbatch, char* out, int len) {

@@ -35,6 +35,16 @@ struct ColArgs {
     int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
     int64_t in_tstr, out_tstr;  // x-tiled input / output: tile (CTA) stride, 0 = x-contiguous
     Prefetch pf;            // column passes 0 / 1 along a short-stride axis
+    // z-slab solves: the column arrays of every rank (device or peer memory)
+    // in place of `out` (mode 0) or `in` (mode 1).  Column x belongs to the
+    // rank j with xs[j] <= x < xs[j + 1]; its value at line index k of outer
+    // index o is col[j][((zs + o) * nl + k) * pitch[j] + x - xs[j]].
+    struct Peers {
+        void* col[8];
+        int xs[9];
+        int64_t pitch[8];
+        int n, zs, nl;
+    } peers;
 };
 
 enum { COL_TILE_DEFAULT = 0, COL_TILE_256 = 1, COL_TILE_128 = 2 };

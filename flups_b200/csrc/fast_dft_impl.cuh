@@ -216,6 +216,16 @@ __device__ __forceinline__ void prefetch_ahead(const Prefetch& pf, int units_per
 
 __device__ __forceinline__ int fold_idx(int i, int M) { return (M > 0 && 2 * i > M) ? M - i : i; }
 
+// element (line index p, outer index o) of column x in the column array of
+// the rank that owns x; lstr: that array's line stride
+template <typename C>
+__device__ __forceinline__ C* peer_column(const ColArgs::Peers& P, int x, int o, int p, int& lstr) {
+    int j = 0;
+    while (j + 1 < P.n && x >= P.xs[j + 1]) ++j;
+    lstr = (int)P.pitch[j];
+    return reinterpret_cast<C*>(P.col[j]) + ((int64_t)(P.zs + o) * P.nl + p) * P.pitch[j] + (x - P.xs[j]);
+}
+
 // asynchronous global -> shared copies (LDGSTS): the stage twiddles and the
 // folded Green's values of a fused pass arrive while the line loads are in
 // flight and the first butterflies run
@@ -367,7 +377,14 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     const int64_t xin = a.in_tstr ? (int64_t)blockIdx.x * a.in_tstr + c : x;
     const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + xin + (int64_t)p * a.in_lstr
                         : reinterpret_cast<const C*>(a.in);
-    const int ls = valid ? F::P * (int)a.in_lstr : 0;
+    int ls = valid ? F::P * (int)a.in_lstr : 0;
+    if constexpr (MODE == 1) {
+        if (a.peers.n > 0 && valid) {
+            int lstr;
+            in = peer_column<C>(a.peers, x, o, p, lstr);
+            ls = F::P * lstr;
+        }
+    }
     C v[R1];
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
@@ -410,7 +427,14 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     if (valid) {
         const int64_t xout = a.out_tstr ? (int64_t)blockIdx.x * a.out_tstr + c : x;
         C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + xout + (int64_t)p * a.out_lstr;
-        const int os = F::P * (int)a.out_lstr;
+        int os = F::P * (int)a.out_lstr;
+        if constexpr (MODE == 0) {
+            if (a.peers.n > 0) {
+                int lstr;
+                out = peer_column<C>(a.peers, x, o, p, lstr);
+                os = F::P * lstr;
+            }
+        }
 #pragma unroll
         for (int r = 0; r < NST; ++r) {
             if (OUTS != SH_ANY || p + F::P * r < a.nout) out[r * os] = v[r];

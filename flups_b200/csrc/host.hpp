@@ -261,6 +261,10 @@ struct Solver {
     bool owned() const { return own[0] >= 0; }
     int slab_own(int z0, int z1, int x0, int x1);
     void* green_share = nullptr;  // allocation of a share's columns of the Green's spectrum
+    // every rank's column array (flups_b200_slab_peers): the y passes of a
+    // share write / read them directly instead of the plane array
+    flb::ColArgs::Peers peers{};
+    int slab_peers(int n, void* const* cols, const int* xs, const int64_t* pitch);
     void slice_green();
     void* work_base(int b) const;
     int slab_check(int type) const;

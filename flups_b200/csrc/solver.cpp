@@ -607,6 +607,13 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         // an x-tiled array is laid out for the 256-thread CTA's width; no tensor map over it
         if (c.in_tstr || c.out_tstr) c.tile = COL_TILE_256;
         else if (prefetch && mode != 2) col_prefetch(c, f64, L, A.ncomp);
+        if (peers.n > 0 && owned() && slab_dim == 2 && A.axis == 1 && mode != 2 && A.ncomp == 1) {
+            // a share's y pass: outputs (forward) or inputs (inverse) in the owners' column arrays
+            c.peers = peers;
+            c.peers.zs = own[0];
+            c.peers.nl = st[ndim - 1].n[1];
+            if (mode == 1) c.pf.nbox = 0;
+        }
         check_cuda(launch_fast_col(f64, mode, L, c, A.ncomp, stream), "column DFT launch");
         return;
     }
@@ -1532,6 +1539,36 @@ int Solver::slab_own(int z0, int z1, int x0, int x1) {
     own[3] = x1;
     const int64_t q = (precision == 64) ? 8 : 16;  // complex values per 128 bytes
     xpitch = (x1 - x0 + q - 1) / q * q;
+    return 0;
+}
+
+// Every rank's column array, for y passes that store their outputs (and
+// load their inputs) there directly: rank j owns columns [xs[j], xs[j+1]),
+// its array has row pitch pitch[j]; this share's own entry must be its
+// column array.  n = 0 goes back to the plane array and the exchanges.
+int Solver::slab_peers(int n, void* const* cols, const int* xs, const int64_t* pitch) {
+    if (!is_setup || !owned()) return -1;
+    if (n == 0) {
+        peers = flb::ColArgs::Peers{};
+        return 0;
+    }
+    if (n < 1 || n > 8 || !cols || !xs || !pitch) return -2;
+    if (xs[0] != 0 || xs[n] != st[ndim - 1].n[0]) return -2;
+    int mine = -1;
+    for (int j = 0; j < n; ++j) {
+        if (xs[j + 1] <= xs[j] || pitch[j] < xs[j + 1] - xs[j] || !cols[j]) return -2;
+        if (xs[j] == own[2] && xs[j + 1] == own[3]) mine = j;
+    }
+    if (mine < 0 || cols[mine] != xbuf || pitch[mine] != xpitch) return -2;
+    flb::ColArgs::Peers P{};
+    for (int j = 0; j < n; ++j) {
+        P.col[j] = cols[j];
+        P.xs[j] = xs[j];
+        P.pitch[j] = pitch[j];
+    }
+    P.xs[n] = xs[n];
+    P.n = n;
+    peers = P;
     return 0;
 }
 

@@ -123,6 +123,10 @@ def load_library(path=None):
         "flups_b200_slab_forward": (c_int, [vp, vp]),
         "flups_b200_slab_fused": (c_int, [vp, c_int]),
         "flups_b200_slab_backward": (c_int, [vp, vp, c_int]),
+        "flups_b200_slab_peers": (c_int, [vp, c_int, POINTER(vp), ip, POINTER(ctypes.c_int64)]),
+        "flups_b200_ipc_handle": (c_int, [vp, vp]),
+        "flups_b200_ipc_open": (c_int, [vp, POINTER(vp)]),
+        "flups_b200_ipc_close": (c_int, [vp]),
         "flups_get_innerBuffer": (vp, [vp]),
         "flups_get_innerTopo_physical": (vp, [vp]),
         "flups_get_innerTopo_spectral": (vp, [vp]),
@@ -346,6 +350,15 @@ class Solver:
 
     def slab_backward(self, field, solver_type=SolverType.STD):
         return _lib.flups_b200_slab_backward(self._solver, _ptr(field), int(solver_type))
+
+    def slab_peers(self, cols, xs, pitches):
+        """Every rank's column array (device addresses), the column split xs (n + 1 values) and
+        the arrays' row pitches; an empty list goes back to the plane array."""
+        n = len(cols)
+        c = (c_void_p * max(1, n))(*[c_void_p(int(p)) for p in cols])
+        x = (c_int * (n + 1))(*[int(v) for v in xs] if n else [0])
+        pt = (ctypes.c_int64 * max(1, n))(*[int(v) for v in pitches])
+        return _lib.flups_b200_slab_peers(self._solver, n, c, x, pt)
 
     def set_col_tile(self, tile):
         """0 default/tuned, 1: 256-thread tiles, 2: 128-thread tiles (cross-checks)."""

@@ -207,6 +207,78 @@ class SlabRank:
         self.backward(field)
 
 
+def _split_table(ranks_or_plan):
+    plan = ranks_or_plan
+    return [a for a, _ in plan.x] + [plan.x[-1][1]]
+
+
+def connect_local(ranks):
+    """Several ranks' solvers in one process (one device): every rank's y
+    passes use the column arrays of all of them directly."""
+    cols = [r.s.slab_columns_ptr() for r in ranks]
+    pitches = [r.columns_shape[2] for r in ranks]
+    for r in ranks:
+        r._ok(r.s.slab_peers(cols, _split_table(r.plan), pitches), "slab_peers")
+
+
+def connect_peers(rank, group=None):
+    """One rank per GPU: open every other rank's column array through CUDA
+    IPC (peer memory over NVLink) so this rank's y passes store into and
+    load from them directly.  Collective over the group."""
+    import ctypes
+
+    import torch.distributed as dist
+    from flups_b200 import pyflups as pf
+    lib = pf.load_library()
+    mine = rank.s.slab_columns_ptr()
+    h = ctypes.create_string_buffer(64)
+    rank._ok(lib.flups_b200_ipc_handle(ctypes.c_void_p(mine), h), "ipc handle")
+    entries = [None] * rank.world
+    dist.all_gather_object(entries, (rank.rank, bytes(h.raw), rank.columns_shape[2]), group=group)
+    cols, pitches, opened = [], [], []
+    for j, hb, pitch in sorted(entries):
+        if j == rank.rank:
+            cols.append(mine)
+        else:
+            ptr = ctypes.c_void_p()
+            rank._ok(lib.flups_b200_ipc_open(ctypes.create_string_buffer(hb, 64), ctypes.byref(ptr)), "ipc open")
+            cols.append(ptr.value)
+            opened.append(ptr.value)
+        pitches.append(pitch)
+    rank._ok(rank.s.slab_peers(cols, _split_table(rank.plan), pitches), "slab_peers")
+    rank._opened = opened
+    return opened
+
+
+def solve_connected(rank, field, rhs, group=None):
+    """The solve of one rank per GPU after connect_peers: the y passes move
+    the spectrum between the GPUs themselves; barriers order the steps."""
+    import torch.distributed as dist
+    torch = rank.torch
+    rank.forward(rhs)
+    torch.cuda.synchronize()
+    dist.barrier(group=group)
+    rank.fused()
+    dist.barrier(group=group)
+    rank.backward(field)
+    torch.cuda.synchronize()
+    dist.barrier(group=group)
+
+
+def solve_local_connected(ranks, fields, rhss):
+    """solve_connected for several ranks' solvers in one process (after connect_local)."""
+    torch = ranks[0].torch
+    for r, rhs in zip(ranks, rhss):
+        r.forward(rhs)
+    torch.cuda.synchronize()
+    for r in ranks:
+        r.fused()
+    torch.cuda.synchronize()
+    for r, f in zip(ranks, fields):
+        r.backward(f)
+    torch.cuda.synchronize()
+
+
 def solve_local(ranks, fields, rhss):
     """The decomposed solve of several ranks' solvers in one process (one
     device): the same steps, with the all-to-all done by device copies."""

@@ -138,6 +138,23 @@ void* flups_b200_slab_columns(struct Solver* s);
 int flups_b200_slab_forward(struct Solver* s, const double* rhs);
 int flups_b200_slab_fused(struct Solver* s, int type);
 int flups_b200_slab_backward(struct Solver* s, double* field, int type);
+/* The column arrays of every rank (n ranks, n <= 8; rank j owns columns
+ * [xs[j], xs[j+1]) with row pitch pitch[j]; this solver's own entry is its
+ * flups_b200_slab_columns array): the y forward pass of flups_b200_slab_forward
+ * then stores each column straight into its owner's array and the y inverse
+ * pass of flups_b200_slab_backward loads it from there, over NVLink for the
+ * arrays of other GPUs (opened with flups_b200_ipc_open), so no exchange
+ * copies remain; the caller only orders the steps across ranks (every
+ * rank's forward before any fused step, every fused step before any
+ * backward, every backward before the next forward).  n = 0 returns to the
+ * plane array.  Returns 0, -1 (not a set-up share) or -2 (bad table). */
+int flups_b200_slab_peers(struct Solver* s, int n, void* const* cols, const int* xs, const int64_t* pitch);
+/* CUDA IPC of a device allocation (cudaIpcGetMemHandle /
+ * cudaIpcOpenMemHandle with lazy peer access / cudaIpcCloseMemHandle); the
+ * handle is 64 bytes.  Return 0, -2 (bad arguments) or -4 (CUDA error). */
+int flups_b200_ipc_handle(const void* dev_ptr, void* handle);
+int flups_b200_ipc_open(const void* handle, void** dev_ptr);
+int flups_b200_ipc_close(void* dev_ptr);
 
 /* A solve (nbatch consecutive right-hand sides, as flups_solve_batch) of
  * device arrays replayed from a CUDA graph.  The first call for a given

@@ -57,6 +57,34 @@ def test_slab_solve_equals_one_rank(n, precision, world, kernel):
         assert r.s.device_bytes(1) < full * (1.0 / world + 0.45)
 
 
+@pytest.mark.parametrize("n,precision,world,kernel", [(64, 64, 2, HEJ_2), (128, 32, 3, LGF_2), (256, 32, 4, LGF_2)])
+def test_slab_connected_equals_one_rank(n, precision, world, kernel):
+    """The y passes store into and load from every rank's column array
+    directly (here all on one GPU): no exchange copies, same result."""
+    import torch
+    from flups_b200.slab import SlabRank, connect_local, solve_local_connected
+    rng = np.random.default_rng(n + 7 * world)
+    rhs = torch.from_numpy(to_user(rng.standard_normal((1, n, n, n)))).cuda()
+    t, s = make_solver([n] * 3, 1, UNB, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, kernel, precision=precision)
+    ref = torch.zeros_like(rhs)
+    s.solve(ref, rhs)
+    torch.cuda.synchronize()
+    keep, ranks = [], []
+    for r in range(world):
+        tr, sr = _unset_solver(n, kernel, precision)
+        keep.append((tr, sr))
+        ranks.append(SlabRank(sr, r, world))
+    connect_local(ranks)
+    rhs_parts = [rhs[0, r.z0:r.z1].contiguous() for r in ranks]
+    for rep in range(2):
+        out_parts = [torch.full_like(p, float("nan")) for p in rhs_parts]
+        solve_local_connected(ranks, out_parts, rhs_parts)
+        assert torch.equal(torch.cat(out_parts).unsqueeze(0), ref), rep
+    assert all(sr.last_error() == 0 for _, sr in keep)
+    # a bad table is refused
+    assert ranks[0].s.slab_peers([0, 0], [0, 1, 2], [1, 1]) == -2
+
+
 def test_slab_refuses_other_problems():
     from flups_b200 import pyflups as pf
     from flups_b200.slab import SlabRank
