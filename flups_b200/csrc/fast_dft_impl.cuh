@@ -24,6 +24,8 @@
 // complex DFT of half length (z_j = x_2j + i x_2j+1).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "cplx.cuh"
 #include "fast_dft.h"
 #include "pass_desc.h"
@@ -773,21 +775,43 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
     const T z = (T)0;
     // real m of the packed line: z_j = (r_{2j}, r_{2j+1}) at line[sw(j)]
     auto slot = [](int m) { return 2 * F::sw(m >> 1) + (m & 1); };
+    auto stage = [&](auto full) {
 #pragma unroll
-    for (int r = 0; r < 2 * R1; ++r) {
-        const int i = p + P * r;
-        const T u = (i < nld) ? (T)src[i] : z;
-        int m;
-        if constexpr (FAM == 2) {
-            m = (i & 1) ? N - 1 - (i >> 1) : (i >> 1);
-        } else if constexpr (FAM == 3) {
-            m = i;
-        } else {
-            const int ii = dst ? N - 1 - i : i;
-            m = (ii & 1) ? N - ii : ii;  // x_{2j} -> r_{2j}; x_{n-1-2j} -> r_{2j+1}
+        for (int r = 0; r < 2 * R1; ++r) {
+            const int i = p + P * r;
+            const T u = (decltype(full)::value || i < nld) ? (T)src[i] : z;
+            if constexpr (FAM == 3 && 64 % P == 0) {
+                // slot(i) = i + 2 (i >> 6), and (p + P r) >> 6 = (P r) >> 6 for p < P | 64
+                lr[p + (P * r + 2 * ((P * r) >> 6))] = u;
+            } else if constexpr (FAM == 2 && P % 2 == 0 && 128 % P == 0) {
+                // i = p + P r has the parity of p: even i -> m = q + (P/2) r, odd i ->
+                // m = N - 1 - (P/2) r - q (q = p >> 1); slot(m) = m + 2 (m >> 6), where q
+                // never carries across a multiple of 64
+                constexpr int H = P / 2;
+                const int q = p >> 1;
+                if (p & 1) {
+                    const int M = N - 1 - H * r;
+                    lr[(M + 2 * (M >> 6)) - q] = dst ? -u : u;
+                } else {
+                    lr[q + (H * r + 2 * ((H * r) >> 6))] = u;
+                }
+            } else {
+                int m;
+                if constexpr (FAM == 2) {
+                    m = (i & 1) ? N - 1 - (i >> 1) : (i >> 1);
+                } else if constexpr (FAM == 3) {
+                    m = i;
+                } else {
+                    const int ii = dst ? N - 1 - i : i;
+                    m = (ii & 1) ? N - ii : ii;  // x_{2j} -> r_{2j}; x_{n-1-2j} -> r_{2j+1}
+                }
+                lr[slot(m)] = (FAM == 2 && dst && (i & 1)) ? -u : u;
+            }
         }
-        lr[slot(m)] = (FAM == 2 && dst && (i & 1)) ? -u : u;
-    }
+    };
+    // rows that hold all N inputs load them without a test per element
+    if (nld >= N) stage(std::true_type{});
+    else stage(std::false_type{});
     cp_async_wait<0>();
     __syncthreads();
     const C* wn = WSM ? wsm : reinterpret_cast<const C*>(a.tw);
@@ -871,7 +895,7 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
         }
     };
     const bool first = a.postpro & PP_NULL_FIRST, last = a.postpro & PP_NULL_LAST, period = a.postpro & PP_ENFORCE_PERIOD;
-    for (int i = p; i < a.nstore; i += P) {
+    auto store = [&](int i) {
         T y;
         if (first && i == 0) y = z;
         else if (last && i == a.nstore - 1) y = z;
@@ -879,6 +903,17 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
         else if (i >= N) y = (i < a.nin) ? (T)src[i] : z;
         else y = value(i);
         out[i] = (OT)y;
+    };
+    if constexpr (FAM == 3) {
+        // outputs i < N as p + P r (compile-time r), then the rest
+#pragma unroll
+        for (int r = 0; r < 2 * R1; ++r) {
+            const int i = p + P * r;
+            if (i < a.nstore) store(i);
+        }
+        for (int i = N + p; i < a.nstore; i += P) store(i);
+    } else {
+        for (int i = p; i < a.nstore; i += P) store(i);
     }
 }
 
