@@ -207,8 +207,8 @@ class SlabRank:
         self.backward(field)
 
 
-def _split_table(ranks_or_plan):
-    plan = ranks_or_plan
+def _split_table(plan):
+    """Column split of the ranks: xs[j] = first column of rank j, xs[world] = columns."""
     return [a for a, _ in plan.x] + [plan.x[-1][1]]
 
 
