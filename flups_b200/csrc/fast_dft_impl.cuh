@@ -84,7 +84,9 @@ __host__ __device__ constexpr int stage_table_entries(int n, int r1) {
 
 // ROWS: the lines of a CTA are thread-index-slow (row passes: p fastest),
 // else thread-index-fast (column passes: the TX columns fastest).
-template <typename T, int L, int R1, bool ROWS = false>
+// GTW: the later-stage table is read from global memory (through L1) even
+// when it is small
+template <typename T, int L, int R1, bool ROWS = false, bool GTW = false>
 struct RegFFT {
     using C = typename CT<T>::C;
     static constexpr int P = L / R1;
@@ -94,7 +96,7 @@ struct RegFFT {
 #ifndef FLB_TW_SMEM_MAX
 #define FLB_TW_SMEM_MAX 8192
 #endif
-    static constexpr bool TWS = TWN > 0 && TWN * (int)sizeof(C) <= FLB_TW_SMEM_MAX;
+    static constexpr bool TWS = !GTW && TWN > 0 && TWN * (int)sizeof(C) <= FLB_TW_SMEM_MAX;
     static constexpr int TW_SMEM = TWS ? TWN : 0;  // complex entries of shared memory for the table
     // line stride in shared memory (complex elements): the swizzled length rounded
     // to 16, plus an offset that puts the lines met by one half-warp on distinct
@@ -340,9 +342,17 @@ __device__ __forceinline__ void stage_green(const ColArgs& a, T* gs, int o) {
 #ifndef FLB_F64_WIDE_THREADS_PER_SM
 #define FLB_F64_WIDE_THREADS_PER_SM 256
 #endif
-template <int THREADS, bool FUSED = false, bool F64_WIDE = false>
+// FP32 forward column passes of power-of-two lines (first radix 32): three
+// 256-thread CTAs per SM at 80 registers, the stage table read through L1
+// so that three CTAs' exchange lines fit in shared memory
+template <typename T, int MODE, int R1>
+struct Fwd3 {
+    static constexpr bool ON = MODE == 0 && R1 == 32 && sizeof(T) == 4;
+};
+
+template <int THREADS, bool FUSED = false, bool F64_WIDE = false, bool THREE = false>
 struct Occ {
-    static constexpr int per_sm = F64_WIDE ? FLB_F64_WIDE_THREADS_PER_SM : (FUSED ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM);
+    static constexpr int per_sm = THREE ? 768 : (F64_WIDE ? FLB_F64_WIDE_THREADS_PER_SM : (FUSED ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM));
     static constexpr int want = per_sm / (THREADS < 64 ? 64 : THREADS);
     static constexpr int blocks = want < 1 ? 1 : want;
 };
@@ -355,8 +365,8 @@ enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
 //      2: forward, Green multiply, inverse (SH: loaded and stored part).
 // The host guarantees L * (line stride) < 2^31 (32-bit offsets along a line).
 template <typename T, int L, int R1, int TX, int MODE, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, sizeof(T) == 8 && (MODE == 2 || R1 == 32)>::blocks)) col_dft_kernel(const __grid_constant__ ColArgs a) {
-    using F = RegFFT<T, L, R1>;
+__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, sizeof(T) == 8 && (MODE == 2 || R1 == 32), Fwd3<T, MODE, R1>::ON && TX * (L / R1) == 256>::blocks)) col_dft_kernel(const __grid_constant__ ColArgs a) {
+    using F = RegFFT<T, L, R1, false, Fwd3<T, MODE, R1>::ON && TX * (L / R1) == 256>;
     using C = typename CT<T>::C;
     constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
     constexpr int OUTS = (MODE == 0) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
@@ -1005,7 +1015,7 @@ cudaError_t launch_colreal_f64(int c2r, int sh, int L, const ColArgs& a, int nco
 
 template <typename T, int L, int R1, int TX, int MODE, int SH>
 inline cudaError_t launch_col_t(const ColArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, L, R1>;
+    using F = RegFFT<T, L, R1, false, Fwd3<T, MODE, R1>::ON && TX * (L / R1) == 256>;
     const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C) +
                         (MODE == 2 ? (size_t)GStage<L>::N * TX * sizeof(T) : 0);
     static std::atomic<unsigned long long> attr{0};
