@@ -350,6 +350,13 @@ struct Fwd3 {
     static constexpr bool ON = MODE == 0 && R1 == 32 && sizeof(T) == 4;
 };
 
+// FP32 r2c rows of power-of-two length: three CTAs per SM at 80 registers,
+// the stage table read through L1 so that three CTAs' lines fit
+template <typename T, int R1>
+struct Row3 {
+    static constexpr bool ON = R1 == 32 && sizeof(T) == 4;
+};
+
 template <int THREADS, bool FUSED = false, bool F64_WIDE = false, bool THREE = false>
 struct Occ {
     static constexpr int per_sm = THREE ? 768 : (F64_WIDE ? FLB_F64_WIDE_THREADS_PER_SM : (FUSED ? FLB_FUSED_THREADS_PER_SM : FLB_COL_THREADS_PER_SM));
@@ -548,8 +555,8 @@ template <> struct Vec2<double> { using V = double2; };
 // IT: type of the real input (the user's double array, or the working precision);
 // HALF: nin = Lh (the row is zero-padded to twice its length)
 template <typename T, typename IT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE>::blocks)) row_r2c_kernel(const __grid_constant__ RowArgs a) {
-    using F = RegFFT<T, LH, R1, true>;
+__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE, Row3<T, R1>::ON>::blocks)) row_r2c_kernel(const __grid_constant__ RowArgs a) {
+    using F = RegFFT<T, LH, R1, true, Row3<T, R1>::ON>;
     using C = typename CT<T>::C;
     using V = typename Vec2<IT>::V;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1189,7 +1196,7 @@ inline cudaError_t launch_dct_types(int f64, int in64, int out64, int n, const R
 
 template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
 inline cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, LH, R1, true>;
+    using F = RegFFT<T, LH, R1, true, !C2R && Row3<T, R1>::ON>;
     constexpr int TR = RowTiles<T, LH, R1>::TR;
     const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + RowTw<T, LH>::N) * sizeof(typename CT<T>::C);
     static std::atomic<unsigned long long> attr{0};
