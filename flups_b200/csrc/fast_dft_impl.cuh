@@ -937,8 +937,8 @@ __global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks))
 // ---------------------------------------------------------------- rows: c2r
 // OT: type of the real output; HALF: nout = Lh (the row is truncated to half)
 template <typename T, typename OT, int LH, int R1, int TR, bool HALF>
-__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE>::blocks)) row_c2r_kernel(const __grid_constant__ RowArgs a) {
-    using F = RegFFT<T, LH, R1, true>;
+__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1), false, RowTiles<T, LH, R1>::WIDE, Row3<T, R1>::ON>::blocks)) row_c2r_kernel(const __grid_constant__ RowArgs a) {
+    using F = RegFFT<T, LH, R1, true, Row3<T, R1>::ON>;
     using C = typename CT<T>::C;
     using V = typename Vec2<OT>::V;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1196,7 +1196,7 @@ inline cudaError_t launch_dct_types(int f64, int in64, int out64, int n, const R
 
 template <typename T, typename XT, int LH, int R1, bool C2R, bool HALF>
 inline cudaError_t launch_row_t(const RowArgs& a, int ncomp, cudaStream_t s) {
-    using F = RegFFT<T, LH, R1, true, !C2R && Row3<T, R1>::ON>;
+    using F = RegFFT<T, LH, R1, true, Row3<T, R1>::ON>;
     constexpr int TR = RowTiles<T, LH, R1>::TR;
     const size_t smem = (size_t)(TR * F::SC + F::TW_SMEM + RowTw<T, LH>::N) * sizeof(typename CT<T>::C);
     static std::atomic<unsigned long long> attr{0};
