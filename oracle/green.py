@@ -11,6 +11,7 @@ from pathlib import Path
 
 import numpy as np
 
+from . import lgf1unb as l1
 from . import specfun as sf
 from .plans import (CHAT_2, HEJ_0, HEJ_2, HEJ_4, HEJ_6, HEJ_8, HEJ_10, LGF_2, LGF_4, LGF_6, LGF_8,
                     MEHR_4F, MEHR_4L, MEHR_6F, MEHR_6L)
@@ -217,6 +218,32 @@ def green_2unb1spe(kind, r, k, ia, ib, ic, length, r_eq2d, r_cut, k_cut):
 
 
 # ------------------------------------------------------ 1 unbounded, 2 spectral
+def _lgf_1unb_other(kind, r, k0, k1, k2, h):
+    """LGF_4/6/8 and MEHR kernels of one unbounded direction
+    (green_kernels.hpp:591-671): the 1-D lattice Green's function at
+    n = round(|r| / h), shifted by the symbol of the spectral wave numbers
+    (one of k0, k1, k2 is zero).  Evaluated once per distinct argument."""
+    r, k0, k1, k2 = np.broadcast_arrays(*(np.asarray(a, dtype=np.float64) for a in (r, k0, k1, k2)))
+    n = np.round(np.abs(r) / h).astype(np.int64)
+    if kind in (LGF_4, LGF_6, LGF_8):
+        sym = {LGF_4: l1.lgf4_symbol, LGF_6: l1.lgf6_symbol, LGF_8: l1.lgf8_symbol}[kind]
+        fn = {LGF_4: l1.lgf4, LGF_6: l1.lgf6, LGF_8: l1.lgf8}[kind]
+        symv = np.vectorize(sym, otypes=[np.float64])
+        c = symv(k0 * h) + symv(k1 * h) + symv(k2 * h)
+        keys = np.stack([n.ravel().astype(np.float64), c.ravel()], axis=1)
+        uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+        vals = np.array([fn(int(a), float(b)) for a, b in uniq])
+    else:
+        fn = {MEHR_4L: l1.meh4_left, MEHR_6L: l1.meh6_left, MEHR_4F: l1.meh4_full, MEHR_6F: l1.meh6_full}[kind]
+        a0, a1, a2 = np.abs(k0), np.abs(k1), np.abs(k2)
+        kmax = np.maximum(a0, np.maximum(a1, a2))
+        kmid = a0 + a1 + a2 - kmax
+        keys = np.stack([n.ravel().astype(np.float64), (kmax * h).ravel(), (kmid * h).ravel()], axis=1)
+        uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+        vals = np.array([fn(int(a), float(b), float(c)) for a, b, c in uniq])
+    return vals[inv.ravel()].reshape(r.shape)
+
+
 def green_1unb2spe(kind, r, k, k0, k1, k2, h, length, k_cut):
     """green_functions.cpp:407-538 (kernels green_kernels.hpp:461-671)."""
     sig = length
@@ -263,10 +290,12 @@ def green_1unb2spe(kind, r, k, k0, k1, k2, h, length, k_cut):
             c = sf.lgf2_symbol(k0 * h) + sf.lgf2_symbol(k1 * h) + sf.lgf2_symbol(k2 * h)
             n = np.round(np.abs(r) / h)
             g = g0 = -h * sf.lgf2_1unb(n, c)
+        elif kind in (LGF_4, LGF_6, LGF_8, MEHR_4L, MEHR_6L, MEHR_4F, MEHR_6F):
+            g = g0 = -h * _lgf_1unb_other(kind, r, k0, k1, k2, h)
         elif kind == HEJ_0:
             raise ValueError("HEJ0 kernel not available for 1D unbounded problems.")
         else:
-            raise NotImplementedError("1-unbounded LGF_4/6/8 and MEHR kernels are not restated in the oracle")
+            raise ValueError("Green Function type unknown.")
     out[m0] = np.asarray(g0 * np.ones_like(r))[m0]
     out[~m0] = np.asarray(g * np.ones_like(r))[~m0]
     return out
