@@ -376,13 +376,12 @@ def vortex_ring_rhs(n, dev):
 
 
 def fast_flags(stats, plan):
-    """Kernel family per timed pass: from the host-side plan where it lists the
-    same passes; the split ROT passes (rot_fwd / rot_curl / rot_bwd) are named."""
+    """Kernel family per timed pass, from the host-side plan of the same passes."""
     planned = [q.get("fast", 0) for q in plan.get("passes", []) if q.get("name") != "green"]
     if len(planned) == len(stats):
         return planned
     by_name = {q.get("name"): q.get("fast", 0) for q in plan.get("passes", [])}
-    return [1 if p["name"] in ("rot_fwd", "rot_bwd", "rot_curl") else by_name.get(p["name"], 0) for p in stats]
+    return [by_name.get(p["name"], 0) for p in stats]
 
 
 def run_config(args):

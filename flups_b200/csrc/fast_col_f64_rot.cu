@@ -1,0 +1,10 @@
+// FP64 ROT column kernels: forward DFT, curl and Green's multiply, inverse DFT (instantiations).
+#include "fast_dft_impl.cuh"
+
+namespace flb {
+
+cudaError_t launch_col_f64_m3(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    return launch_rot_shape<double>(sh, L, a, ncomp, s);
+}
+
+}  // namespace flb

@@ -85,6 +85,7 @@ cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncom
     if (mode == 0) sh = (a.nout == L) ? shape(a.nin) : SH_ANY;
     else if (mode == 1) sh = (a.nin == L) ? shape(a.nout) : SH_ANY;
     else sh = (shape(a.nin) == shape(a.nout)) ? shape(a.nin) : SH_ANY;
+    if (mode == 3) return f64 ? launch_col_f64_m3(sh, L, a, ncomp, s) : launch_col_f32_m3(sh, L, a, ncomp, s);
     if (f64) return (mode == 2) ? launch_col_f64_m2(sh, L, a, ncomp, s) : launch_col_f64_m01(mode, sh, L, a, ncomp, s);
     if (mode == 2) return launch_col_f32_m2(sh, L, a, ncomp, s);
     return launch_col_f32_m01(mode, sh, L, a, ncomp, s);

@@ -33,8 +33,14 @@ struct ColArgs {
     double normfact;
     int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
     int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
-    int64_t in_tstr, out_tstr;  // x-tiled input / output: tile (CTA) stride, 0 = x-contiguous
     Prefetch pf;            // column passes 0 / 1 along a short-stride axis
+    // ROT fused pass (mode 3): the curl's wave-number symbols K_{d,c}(i), one
+    // table of complex working-precision values per direction d and component
+    // c at ksym + (3 d + c) kstr, indexed by the spectral index along d; the
+    // directions of the line and of the outer index
+    const void* ksym;
+    int kstr;
+    int ax_line, ax_outer;
     // z-slab solves: the column arrays of every rank (device or peer memory)
     // in place of `out` (mode 0) or `in` (mode 1).  Column x belongs to the
     // rank j with xs[j] <= x < xs[j + 1]; its value at line index k of outer
@@ -104,9 +110,10 @@ __host__ __device__ constexpr bool fast_radix48(int n, int f64) { return !f64 &&
 __host__ __device__ constexpr int fast_radix1_row(int n, int f64) {
     return fast_radix48(n, f64) ? 48 : ((f64 && n % 3 != 0) ? 32 : fast_radix1_of(n, f64));
 }
-// column c2c passes of mode 0 (forward), 1 (inverse) or 2 (fused: radix 48 not used)
+// column c2c passes of mode 0 (forward), 1 (inverse), 2 (fused) or 3 (fused
+// ROT); radix 48 not used by the fused passes
 __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
-    return (mode != 2 && fast_radix48(n, f64)) ? 48 : ((n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
+    return (mode < 2 && fast_radix48(n, f64)) ? 48 : ((n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
 }
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix
@@ -134,6 +141,9 @@ __host__ __device__ inline void fast_stage_exponent(int n, int r1, int e, int* q
     *q = (int)(((long long)r * k) % (Ns * Rs));
 }
 
+// column c2c pass of mode 0 (forward DFT), 1 (inverse DFT), 2 (forward,
+// Green's multiply, inverse) or 3 (forward, curl and Green's multiply of
+// groups of three components, inverse)
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 // r2r rows (DCT / DST I-IV) through an M-point complex register DFT

@@ -392,9 +392,7 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     T* gs = reinterpret_cast<T*>(sm + TX * F::SC + F::TW_SMEM);
     if constexpr (MODE == 2) stage_green<T, L, TX>(a, gs, o);
     // lanes outside the array read its first element and drop it (no branch)
-    // x-tiled arrays: column c of CTA blockIdx.x at blockIdx.x * tstr + c
-    const int64_t xin = a.in_tstr ? (int64_t)blockIdx.x * a.in_tstr + c : x;
-    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + xin + (int64_t)p * a.in_lstr
+    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
                         : reinterpret_cast<const C*>(a.in);
     int ls = valid ? F::P * (int)a.in_lstr : 0;
     if constexpr (MODE == 1) {
@@ -444,8 +442,7 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
         F::template fft<false, true>(v, line, p, tws + zero);
     }
     if (valid) {
-        const int64_t xout = a.out_tstr ? (int64_t)blockIdx.x * a.out_tstr + c : x;
-        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + xout + (int64_t)p * a.out_lstr;
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
         int os = F::P * (int)a.out_lstr;
         if constexpr (MODE == 0) {
             if (a.peers.n > 0) {
@@ -457,6 +454,139 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
 #pragma unroll
         for (int r = 0; r < NST; ++r) {
             if (OUTS != SH_ANY || p + F::P * r < a.nout) out[r * os] = v[r];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- columns, ROT
+// The curl and Green's multiply of a ROT solve fused between the forward and
+// inverse DFT of the last direction (dothemagic_rot.ipp:102-350 between the
+// transforms of Solver.cpp:1402-1462): the three components of TX columns
+// meet in one CTA, one group of TX x P threads per component.  After the
+// forward DFT every group puts its spectrum in its own exchange lines, reads
+// the other two components at the same wave numbers, forms its component of
+// G (i K x w),
+//   u_g = G (w_{g+2} K_{g+1,g+2} - w_{g+1} K_{g+2,g+1})  (indices mod 3),
+// and transforms it back.  K_{d,c} is read from per-direction tables (the
+// spectral or finite-difference symbol with the phase of the derivative);
+// along the line it changes with the wave number, along x and the outer
+// direction it is one value per thread.
+template <typename T, int L>
+struct RotTile {
+    static constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, 2);
+    static constexpr int P = L / R1;
+    // threads per component group: 128, or 64 for the FP64 lines of first
+    // radix 32 (up to 255 registers).  Measured at 384^3 (768-point lines,
+    // FP32): 5.90 ms with 128, 6.66 ms with 64 at two CTAs per SM (16-byte
+    // row segments)
+#ifndef FLB_ROT_GROUP
+#define FLB_ROT_GROUP 128
+#endif
+    static constexpr int GROUP = (sizeof(T) == 8 && R1 == 32) ? FLB_ROT_GROUP / 2 : FLB_ROT_GROUP;
+    static constexpr int TX = P >= GROUP ? 1 : GROUP / P;
+    static constexpr int THREADS = 3 * TX * P;
+};
+#ifndef FLB_ROT_MINB
+#define FLB_ROT_MINB 1
+#endif
+
+template <typename T, int L, int R1, int TX, int SH>
+__global__ void __launch_bounds__(3 * TX * (L / R1), FLB_ROT_MINB) col_rot_kernel(const __grid_constant__ ColArgs a) {
+    using F = RegFFT<T, L, R1>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P, GT = TX * P;
+    constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;  // registers loaded
+    constexpr int NST = NLD;                             // registers stored
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int g = threadIdx.x / GT, t = threadIdx.x % GT;  // component group; thread in it
+    const int c = t % TX, p = t / TX;
+    const int x = blockIdx.x * TX + c;
+    const int o = mirror_order(blockIdx.y, a.nouter, a.f_outer);
+    const int comp = 3 * blockIdx.z + g;
+    const bool valid = x < a.nx;
+    const C* tws = stage_twiddles<F>(a.tws, sm + 3 * TX * F::SC);
+    T* gs = reinterpret_cast<T*>(sm + 3 * TX * F::SC + F::TW_SMEM);
+    stage_green<T, L, TX>(a, gs, o);
+    // lanes outside the array read its first element and drop it (no branch)
+    const C* in = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+                        : reinterpret_cast<const C*>(a.in);
+    const int ls = valid ? P * (int)a.in_lstr : 0;
+    C v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        if (r >= NLD) {
+            v[r] = mkc((T)0, (T)0);
+        } else if constexpr (SH != SH_ANY) {
+            v[r] = in[r * ls];
+        } else {
+            const bool ok = valid && p + P * r < a.nin;
+            const C u = in[ok ? r * ls : 0];
+            v[r] = ok ? u : mkc((T)0, (T)0);
+        }
+    }
+    if constexpr (F::TWS) cp_async_wait<1>();
+    C* line = sm + (g * TX + c) * F::SC;
+    F::template fft<SH == SH_HALF, false>(v, line, p, tws);
+    // the two symbols of this group: K_a = K_{g+1, g+2} multiplies w_{g+2},
+    // K_b = K_{g+2, g+1} multiplies w_{g+1}; at most one of them runs along the line
+    const int ga = (g + 2) % 3, gb = (g + 1) % 3;
+    const C* K = reinterpret_cast<const C*>(a.ksym);
+    const int xi = valid ? x : 0;
+    auto at = [&](int d) { return d == 0 ? xi : o; };
+    const C* ktab = nullptr;
+    int vary = 0;  // 1: K_a along the line, 2: K_b along the line
+    C ka = mkc((T)0, (T)0), kb = mkc((T)0, (T)0);
+    if (gb == a.ax_line) {
+        vary = 1;
+        ktab = K + (3 * gb + ga) * a.kstr;
+    } else {
+        ka = K[(3 * gb + ga) * a.kstr + at(gb)];
+    }
+    if (ga == a.ax_line) {
+        vary = 2;
+        ktab = K + (3 * ga + gb) * a.kstr;
+    } else {
+        kb = K[(3 * ga + gb) * a.kstr + at(ga)];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    __syncthreads();
+    {
+        const C* fa = sm + (ga * TX + c) * F::SC;
+        const C* fb = sm + (gb * TX + c) * F::SC;
+        // k = p + P r; fold(k) = k for r < R1/2, L - k above (k = L/2 included);
+        // the stored spectrum already carries the normalisation
+        const T* g0 = gs + p * TX + c;
+        const T* g1 = gs + (L - p) * TX + c;
+        auto curl = [&](auto mode) {
+            constexpr int VARY = decltype(mode)::value;
+#pragma unroll
+            for (int r = 0; r < R1; ++r) {
+                const int k = p + P * r;
+                const C A = (VARY == 1) ? __ldg(ktab + k) : ka;
+                const C B = (VARY == 2) ? __ldg(ktab + k) : kb;
+                const C u = csub(cmul(fa[F::sw(k)], A), cmul(fb[F::sw(k)], B));
+                v[r] = cscale(u, r < R1 / 2 ? g0[r * P * TX] : g1[-r * P * TX]);
+            }
+        };
+        if (vary == 1) curl(std::integral_constant<int, 1>{});
+        else if (vary == 2) curl(std::integral_constant<int, 2>{});
+        else curl(std::integral_constant<int, 0>{});
+    }
+    // every group has read the others' spectra before the inverse DFT reuses the lines
+    __syncthreads();
+    int zero = 0;
+    asm("" : "+r"(zero));
+    F::template fft<false, true>(v, line, p, tws + zero);
+    if (valid) {
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int os = P * (int)a.out_lstr;
+#pragma unroll
+        for (int r = 0; r < NST; ++r) {
+            if (SH != SH_ANY || p + P * r < a.nout) out[r * os] = v[r];
         }
     }
 }
@@ -1012,6 +1142,8 @@ cudaError_t launch_col_f32_m01(int mode, int sh, int L, const ColArgs& a, int nc
 cudaError_t launch_col_f32_m2(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f64_m01(int mode, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f64_m2(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_col_f32_m3(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_col_f64_m3(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_row_units(int f64, int c2r, int xt64, bool half, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_r2r_units(int f64, int in64, int out64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
@@ -1073,6 +1205,51 @@ inline cudaError_t launch_col_mode(int L, const ColArgs& a, int ncomp, cudaStrea
         case 1536: return wide ? launch_col_threads<T, 1536, 256, MODE, SH>(a, ncomp, s) : launch_col_threads<T, 1536, 128, MODE, SH>(a, ncomp, s);
     }
     return cudaErrorInvalidValue;
+}
+
+// ROT fused pass: ncomp = 3 x (groups of three components)
+template <typename T, int L, int SH>
+inline cudaError_t launch_rot_t(const ColArgs& a, int ncomp, cudaStream_t s) {
+    using RT = RotTile<T, L>;
+    using F = RegFFT<T, L, RT::R1>;
+    constexpr size_t smem =
+        (size_t)(3 * RT::TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C) + (size_t)GStage<L>::N * RT::TX * sizeof(T);
+    if constexpr (smem > 227 * 1024) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (ncomp % 3 != 0 || ncomp / 3 > 65535) return cudaErrorInvalidValue;
+        static std::atomic<unsigned long long> attr{0};
+        if (cudaError_t e = smem_attr_once(attr, col_rot_kernel<T, L, RT::R1, RT::TX, SH>, smem); e != cudaSuccess) return e;
+        dim3 grid((a.nx + RT::TX - 1) / RT::TX, a.nouter, ncomp / 3);
+        col_rot_kernel<T, L, RT::R1, RT::TX, SH><<<grid, RT::THREADS, smem, s>>>(a);
+        return cudaGetLastError();
+    }
+}
+
+template <typename T, int SH>
+inline cudaError_t launch_rot_len(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    switch (L) {
+        case 48: return launch_rot_t<T, 48, SH>(a, ncomp, s);
+        case 64: return launch_rot_t<T, 64, SH>(a, ncomp, s);
+        case 96: return launch_rot_t<T, 96, SH>(a, ncomp, s);
+        case 128: return launch_rot_t<T, 128, SH>(a, ncomp, s);
+        case 192: return launch_rot_t<T, 192, SH>(a, ncomp, s);
+        case 256: return launch_rot_t<T, 256, SH>(a, ncomp, s);
+        case 384: return launch_rot_t<T, 384, SH>(a, ncomp, s);
+        case 512: return launch_rot_t<T, 512, SH>(a, ncomp, s);
+        case 768: return launch_rot_t<T, 768, SH>(a, ncomp, s);
+        case 1024: return launch_rot_t<T, 1024, SH>(a, ncomp, s);
+        case 1536: return launch_rot_t<T, 1536, SH>(a, ncomp, s);
+        case 2048: return launch_rot_t<T, 2048, SH>(a, ncomp, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T>
+inline cudaError_t launch_rot_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
+    if (sh == SH_FULL) return launch_rot_len<T, SH_FULL>(L, a, ncomp, s);
+    if (sh == SH_HALF) return launch_rot_len<T, SH_HALF>(L, a, ncomp, s);
+    return launch_rot_len<T, SH_ANY>(L, a, ncomp, s);
 }
 
 template <typename T, int L, bool C2R, int SH>

@@ -5,6 +5,7 @@
 #include <math_constants.h>
 
 #include "green.cuh"
+#include "lgf1unb.cuh"
 
 namespace flb {
 
@@ -327,13 +328,24 @@ __device__ double g_1unb2spe(const GreenEvalArgs& A, double r, double k, double 
     const bool zk = k <= A.k_cut;
     if (is_hej(kind)) return hej_1unb(kind, r, k, A.length, zk);
     if (kind == G_CHAT_2) return zk ? 0.5 * fabs(r) : -0.5 * exp(-k * r) / k;
-    if (kind == G_LGF_2) {
-        const double h = A.hgrid;
-        const double c = lgf2_symbol(ka * h) + lgf2_symbol(kb * h) + lgf2_symbol(kc * h);
-        const int n = (int)round(fabs(r) / h);
-        return -h * lgf2_1unb_d(n, c);
+    const double h = A.hgrid;
+    const int n = (int)round(fabs(r) / h);
+    switch (kind) {
+        case G_LGF_2: return -h * lgf2_1unb_d(n, lgf2_symbol(ka * h) + lgf2_symbol(kb * h) + lgf2_symbol(kc * h));
+        case G_LGF_4: return -h * lgf1::lgf4(n, lgf4_symbol(ka * h) + lgf4_symbol(kb * h) + lgf4_symbol(kc * h));
+        case G_LGF_6: return -h * lgf1::lgf6(n, lgf6_symbol(ka * h) + lgf6_symbol(kb * h) + lgf6_symbol(kc * h));
+        case G_LGF_8: return -h * lgf1::lgf8(n, lgf8_symbol(ka * h) + lgf8_symbol(kb * h) + lgf8_symbol(kc * h));
     }
-    return 0.0;  // not reached: the host refuses the other kernels in this splitting
+    // Mehrstellen: one of the wave numbers is zero; |k1| >= |k2| >= 0
+    const double k1 = fmax(fabs(ka), fmax(fabs(kb), fabs(kc)));
+    const double k2 = fabs(ka) + fabs(kb) + fabs(kc) - k1;
+    switch (kind) {
+        case G_MEHR_4L: return -h * lgf1::meh4(n, k1 * h, k2 * h, false);
+        case G_MEHR_4F: return -h * lgf1::meh4(n, k1 * h, k2 * h, true);
+        case G_MEHR_6L: return -h * lgf1::meh6(n, k1 * h, k2 * h, false);
+        case G_MEHR_6F: return -h * lgf1::meh6(n, k1 * h, k2 * h, true);
+    }
+    return 0.0;  // not reached: HEJ_0 is refused by the host in this splitting
 }
 
 __device__ double g_0unb3spe(int kind, double ksqr, double k0, double k1, double k2, double h, double sig) {

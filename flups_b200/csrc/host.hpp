@@ -215,7 +215,6 @@ struct Solver {
     void run_pass(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64, const char* name = "pass");
     int timed_begin(const char* name, double bytes);
     void timed_end(int k);
-    bool rot_split(int nbatch);
     // ---------------------------------------------------------------- advanced API (flups.h:473-578)
     size_t inner_elems = 0;               // doubles in the inner buffer
     int64_t inner_pitch = 0;              // complex row pitch of the spectral layout
@@ -224,8 +223,11 @@ struct Solver {
     void adv_copy(const Topology* topo, double* data, int sign);
     void adv_fft(double* data, int sign);
     void adv_mult(double* data, int type);
-    void* spec_buf = nullptr;             // full spectrum of a split ROT solve
-    size_t spec_bytes = 0;
+    // curl symbols of the fused ROT pass: K_{d,c}(i) per direction d and
+    // component c, kstr complex values each (working precision), built at set-up
+    void* ksym = nullptr;
+    int kstr = 0;
+    void build_ksym();
     void collect_timing();
     void check_cuda(cudaError_t e, const char* what);
     void do_fft_forward(const double* user_in, int nbatch);
@@ -265,6 +267,7 @@ struct Solver {
     // share write / read them directly instead of the plane array
     flb::ColArgs::Peers peers{};
     int slab_peers(int n, void* const* cols, const int* xs, const int64_t* pitch);
+    bool slab_y_fast();
     void slice_green();
     void* work_base(int b) const;
     int slab_check(int type) const;

@@ -1,15 +1,14 @@
 // flups_solve_noalloc: a solve that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc while they run: code being captured
-// into a CUDA graph in the global capture mode (allocation calls are refused
-// there), real-time loops that must stay out of the allocator (cudaMalloc can
-// synchronise the device and takes driver locks), and frameworks that reserve
-// the device memory for their own pools up front, so that a late cudaMalloc
-// fails.  For them this entry point runs one solve of an already set-up
-// solver with all of its per-solve scratch -- the two work arrays between the
-// line passes and the twiddle tables of those passes -- in one file-scope
-// device array of FLUPS_NOALLOC_SCRATCH_BYTES (64 MiB).  Every GPU that loads
-// the library holds that array until the process exits.
+// Some callers cannot call cudaMalloc while they run: real-time loops that
+// must stay out of the allocator (cudaMalloc can synchronise the device and
+// takes driver locks, so its latency has no bound), and frameworks that
+// reserve the device memory for their own pools at start-up, after which a
+// late cudaMalloc fails.  For them this entry point runs one solve of an
+// already set-up solver with all of its per-solve scratch -- the two work
+// arrays between the line passes and the twiddle tables of those passes -- in
+// one file-scope device array of FLUPS_NOALLOC_SCRATCH_BYTES (64 MiB).  Every
+// GPU that loads the library holds that array until the process exits.
 //
 // Rules for callers:
 //   - field and rhs must be device pointers: there is no host staging;
@@ -181,49 +180,65 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
     }
 
     cudaStream_t st = s->stream;
+    // launch-time lookups find the slots planned above; a key that planning did
+    // not place is an error (checked before anything is launched), never a new
+    // slot past the size check
+    bool missing = false;
+    auto tw_of = [&](int n, int stage) -> const void* {
+        for (const TwSlot& t : slots)
+            if (t.n == n && t.stage == stage) return base + t.off;
+        missing = true;
+        return nullptr;
+    };
+    // go = false: resolve every table of every pass without launching
+    auto run = [&](bool go) -> cudaError_t {
+        for (size_t i = 0; i < passes.size(); ++i) {
+            PassArgs A = passes[i];
+            const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
+            cudaError_t e = cudaSuccess;
+            if (kinds[i] == 0) {
+                for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M, 0);
+                if (go) e = launch_line_pass(A, f64 ? 1 : 0, in64 ? 1 : 0, out64 ? 1 : 0, st);
+            } else {
+                const int L = A.st[0].M;
+                ColArgs c;
+                RowArgs r;
+                int mode = 0;
+                s->fast_args(A, kinds[i], in64, out64, c, r, mode);
+                if (kinds[i] == 1) {
+                    c.tws = tw_of(L, fast_radix1_mode(L, f64 ? 1 : 0, mode));
+                    if (go) e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
+                } else if (kinds[i] == 3) {
+                    c.tws = tw_of(L, r1_of(L));
+                    if (go) e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
+                } else if (kinds[i] == 4) {
+                    r.tw2 = tw_of(2 * L, 0);
+                    if (fast_dct_family(r.kind, r.n, L)) {
+                        r.tw = tw_of(r.n, 0);
+                        r.tws = tw_of(r.n / 2, r1_of(r.n / 2));
+                    } else {
+                        r.tws = tw_of(L, r1_of(L));
+                    }
+                    if (go) e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
+                } else {
+                    r.tw = tw_of(L, 0);
+                    r.tws = tw_of(L / 2, fast_radix1_row(L / 2, f64 ? 1 : 0));
+                    if (go) e = launch_fast_row(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, st);
+                }
+            }
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    run(false);
+    if (missing) return fail(-4, "a pass needs a twiddle table that was not planned (internal error)");
     for (const TwSlot& t : slots) {
         const int nb = std::min(1184, (t.len + 255) / 256);
         noalloc_twiddle_kernel<<<nb, 256, 0, st>>>(base + t.off, t.n, t.stage, t.len, t.stage, f64 ? 1 : 0);
     }
-    auto tw_of = [&](int n, int stage) { return (const void*)(base + slot_for(n, stage)); };
-    for (size_t i = 0; i < passes.size(); ++i) {
-        PassArgs& A = passes[i];
-        const bool in64 = flags[i] & 2, out64 = flags[i] & 4;
-        cudaError_t e = cudaSuccess;
-        if (kinds[i] == 0) {
-            for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M, 0);
-            e = launch_line_pass(A, f64 ? 1 : 0, in64 ? 1 : 0, out64 ? 1 : 0, st);
-        } else {
-            const int L = A.st[0].M;
-            ColArgs c;
-            RowArgs r;
-            int mode = 0;
-            s->fast_args(A, kinds[i], in64, out64, c, r, mode);
-            if (kinds[i] == 1) {
-                c.tws = tw_of(L, fast_radix1_mode(L, f64 ? 1 : 0, mode));
-                e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
-            } else if (kinds[i] == 3) {
-                c.tws = tw_of(L, r1_of(L));
-                e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
-            } else if (kinds[i] == 4) {
-                r.tw2 = tw_of(2 * L, 0);
-                if (fast_dct_family(r.kind, r.n, L)) {
-                    r.tw = tw_of(r.n, 0);
-                    r.tws = tw_of(r.n / 2, r1_of(r.n / 2));
-                } else {
-                    r.tws = tw_of(L, r1_of(L));
-                }
-                e = launch_fast_r2r(f64 ? 1 : 0, L, r, A.ncomp, st);
-            } else {
-                r.tw = tw_of(L, 0);
-                r.tws = tw_of(L / 2, fast_radix1_row(L / 2, f64 ? 1 : 0));
-                e = launch_fast_row(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, r, A.ncomp, st);
-            }
-        }
-        if (e != cudaSuccess) {
-            s->last_error = (int)e;
-            return fail(-4, cudaGetErrorString(e));
-        }
+    if (const cudaError_t e = run(true); e != cudaSuccess) {
+        s->last_error = (int)e;
+        return fail(-4, cudaGetErrorString(e));
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -93,9 +93,6 @@ struct PassArgs {
     LineStage st[2];
     MultSpec mult;
     int nlines;                  // number of line positions (n_a * n_b)
-    // x-tiled arrays (register-DFT column passes only): element x sits at
-    // (x / w) * tstr + x % w along x, w = the columns of one CTA; 0 = x-contiguous
-    int64_t in_tstr, out_tstr;
 };
 
 }  // namespace flb

@@ -14,13 +14,14 @@ struct RotArgs {
     int64_t cstr;        // component stride
     int nbatch;          // ROT: groups of 3 components
     int ncomp;           // STD: components multiplied
-    int64_t tstr;        // x-tiled spectrum: x at (x / tw) * tstr + x % tw (tstr = 0: x * str[0])
-    int tw;
     MultSpec mult;       // mode 1 (STD) or 2 (ROT): Green, folds, wave-number tables, derivative order
 };
 
-cudaError_t launch_rot_mult(const RotArgs& A, int f64, cudaStream_t s);
 // data in FP64 or the working precision, Green in the working precision
 cudaError_t launch_spec_mult(const RotArgs& A, int data_f64, int green_f64, cudaStream_t s);
+// the curl's wave-number symbols K_{d,c}(i), i < n[d], of a ROT multiply
+// (mode 2 MultSpec), table (d, c) at out + (3 d + c) kstr complex values of
+// the working precision
+cudaError_t launch_ksym_table(const MultSpec& G, const int n[3], int kstr, void* out, int f64, cudaStream_t s);
 
 }  // namespace flb

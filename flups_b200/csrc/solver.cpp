@@ -179,7 +179,7 @@ Solver::~Solver() {
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
     if (stage_out) cudaFree(stage_out);
-    if (spec_buf) cudaFree(spec_buf);
+    if (ksym) cudaFree(ksym);
     if (h2d_stream) {
         for (int k = 0; k < kSlabs; ++k) {
             cudaEventDestroy(ev_in[k]);
@@ -420,7 +420,11 @@ MultSpec Solver::mult_spec(int type) const {
 
 // Which register-resident kernel can run this pass (0 = none: the general line pass).
 int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) const {
-    if (!use_fast || A.comps_together) return 0;
+    if (!use_fast) return 0;
+    // components together: only the fused ROT pass (groups of three components)
+    const bool rot = A.fused && A.mult.mode == 2;
+    if (A.comps_together && !(rot && A.lda == 3 && A.ncomp % 3 == 0 && ksym)) return 0;
+    if (rot && !A.comps_together) return 0;
     if (A.n_b > 65535 || A.ncomp > 65535) return 0;  // grid y / z limits of the fast launches
     // vector loads/stores of complex (or real pairs) need their natural alignment
     const uintptr_t ain = dry ? 0 : (uintptr_t)A.in, aout = dry ? 0 : (uintptr_t)A.out;
@@ -486,7 +490,7 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
     if (A.axis != 0) {
         // columns: complex DFT, working precision in and out, x contiguous
         if (k0 != LK_C2C || !S0.in_cplx || !S0.out_cplx || in_f64 != f64 || out_f64 != f64) return 0;
-        if (A.fused && (A.st[1].spec[0].kind != LK_C2C || A.st[1].M != S0.M || A.mult.mode != 1)) return 0;
+        if (A.fused && (A.st[1].spec[0].kind != LK_C2C || A.st[1].M != S0.M || (A.mult.mode != 1 && !rot))) return 0;
         if (A.fused && (A.mult.gfold[A.axis] != S0.M || (int64_t)S0.M * A.mult.gstr[A.axis] >= (int64_t)INT32_MAX)) return 0;
         if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
         const int L = S0.M;
@@ -537,11 +541,15 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
         c.out_lstr = A.out_str[A.axis];
         c.out_ostr = A.out_str[b];
         c.out_cstr = A.out_cstr;
-        c.in_tstr = A.in_tstr;
-        c.out_tstr = A.out_tstr;
         mode = (S0.spec[0].sign > 0) ? 1 : 0;
         if (A.fused) {
-            mode = 2;
+            mode = (A.mult.mode == 2) ? 3 : 2;
+            if (mode == 3) {
+                c.ksym = ksym;
+                c.kstr = kstr;
+                c.ax_line = A.axis;
+                c.ax_outer = b;
+            }
             c.green = A.mult.green;
             c.g_x = A.mult.gstr[0];
             c.g_line = A.mult.gstr[A.axis];
@@ -604,10 +612,8 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
             auto it = tuned_tile.find(pass_key(A, f64));
             if (it != tuned_tile.end()) c.tile = it->second;
         }
-        // an x-tiled array is laid out for the 256-thread CTA's width; no tensor map over it
-        if (c.in_tstr || c.out_tstr) c.tile = COL_TILE_256;
-        else if (prefetch && mode != 2) col_prefetch(c, f64, L, A.ncomp);
-        if (peers.n > 0 && owned() && slab_dim == 2 && A.axis == 1 && mode != 2 && A.ncomp == 1) {
+        if (prefetch && mode < 2) col_prefetch(c, f64, L, A.ncomp);
+        if (peers.n > 0 && owned() && slab_dim == 2 && A.axis == 1 && mode < 2 && A.ncomp == 1) {
             // a share's y pass: outputs (forward) or inputs (inverse) in the owners' column arrays
             c.peers = peers;
             c.peers.zs = own[0];
@@ -741,6 +747,9 @@ void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, 
         dry_fast.push_back(fk);
         return;
     }
+    // a connected share's y passes must reach the owners' column arrays
+    FLB_CHECK(!(peers.n > 0 && owned() && slab_dim == 2 && A.axis == 1 && !A.fused) || (fk == 1 && A.ncomp == 1),
+              "a share connected to its peers' column arrays needs register-DFT y passes");
     for (int s2 = 0; s2 <= A.fused; ++s2)
         if (!A.st[s2].tw) A.st[s2].tw = twiddle(A.st[s2].M, f64);
     // algorithmic bytes: source and kept output lines once, the folded Green's spectrum once
@@ -751,8 +760,6 @@ void Solver::run_pass(const PassArgs& Ain, bool f64, bool in_f64, bool out_f64, 
                    (double)last.n_store * A.nlines * nc * (last.out_cplx ? 2 : 1) * (out_f64 ? 8.0 : 4.0);
     if (A.fused) bytes += (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
     const int k = timed_begin(name, bytes);
-    // x-tiled arrays exist only between the register-DFT column passes of the ROT split
-    FLB_CHECK(fk == 1 || (A.in_tstr == 0 && A.out_tstr == 0), "x-tiled array outside a register-DFT column pass");
     if (fk) launch_fast(A, fk, f64, in_f64, out_f64);
     else check_cuda(launch_line_pass(A, f64 ? 1 : 0, in_f64 ? 1 : 0, out_f64 ? 1 : 0, stream), "line pass launch");
     timed_end(k);
@@ -911,8 +918,6 @@ void Solver::compute_green() {
         }
     } else if (nunb == 1) {
         FLB_CHECK(kind != HEJ_0, "HEJ0 kernel not available for 1D unbounded problems.");
-        FLB_CHECK(is_hej || kind == CHAT_2 || kind == LGF_2,
-                  "kernel %d with one unbounded direction is not supported by this library yet", kind);
         E.k_cut = (kfact[E.ax[0]] + kfact[E.ax[1]] + kfact[E.ax[2]]) * 0.2;
         E.hgrid = hfact[E.ax[0]] + hfact[E.ax[1]] + hfact[E.ax[2]];
     } else {
@@ -1051,8 +1056,28 @@ void Solver::setup() {
               cudaGetErrorString(e));
     compute_green();
     if (owned()) slice_green();
+    build_ksym();
     ensure_buffers(1);
     is_setup = true;
+}
+
+// The curl symbols K_{d,c}(i) of a solver that can run ROT (three components
+// and a derivative order), for the fused ROT column pass: 9 tables of the
+// spectral extents, evaluated on the device with the functions of the
+// pointwise multiply.
+void Solver::build_ksym() {
+    if (!have_diff || lda != 3 || dry || ksym) return;
+    const MultSpec G = mult_spec(ROT);
+    int n[3];
+    kstr = 1;
+    for (int d = 0; d < 3; ++d) {
+        n[d] = st[ndim].n[d];
+        kstr = std::max(kstr, n[d]);
+    }
+    const bool f64 = (precision == 64);
+    check_cuda(cudaMalloc(&ksym, (size_t)9 * kstr * 2 * (f64 ? 8 : 4)), "curl symbol tables");
+    check_cuda(launch_ksym_table(G, n, kstr, ksym, f64 ? 1 : 0, stream), "curl symbol tables");
+    check_cuda(cudaStreamSynchronize(stream), "curl symbol tables");
 }
 
 // A solver set up for a share keeps only its columns [own[2], own[3]) of the
@@ -1128,6 +1153,7 @@ size_t Solver::device_bytes(int nbatch) const {
     if (owned()) total += (size_t)xpitch * st[ndim - 1].n[1] * st[ndim - 1].n[2] * 2 * es;
     // (a share holds its columns of the Green's spectrum: gstr describes that array after set-up)
     total += (size_t)gstr[2] * gfold_n[2] * es;
+    if (ksym) total += (size_t)9 * kstr * 2 * es;
     return total;
 }
 
@@ -1169,87 +1195,10 @@ void Solver::do_fft_backward_fused(double* user_out, int type, int nbatch) {
     do_backward(user_out, type, nbatch);
 }
 
-// ROT with the register DFTs on the last direction: forward DFT of the three
-// components into the full spectrum, the pointwise curl and Green's multiply
-// (rot.cu), inverse DFT back.  The general fused pass does the same on lines
-// in shared memory; splitting it lets both transforms run at the DFTs' speed
-// at the price of writing and reading the spectrum once.
-bool Solver::rot_split(int nbatch) {
-    if (dry || !use_fast || slab_dim >= 0) return false;
-    const bool f64 = (precision == 64);
-    const int es = f64 ? 8 : 4;
-    const int ipl = ndim - 1;
-    const DirPlan& p = fwd[ipl];
-    PassArgs F = base_pass(p.dim, st[ipl], lda * nbatch, lda);
-    F.st[0] = stage_forward(p, ipl, f64);
-    set_strides_internal(F.in_str, F.in_cstr, st[ipl]);
-    set_strides_internal(F.out_str, F.out_cstr, st[ndim]);
-    PassArgs Bk = base_pass(p.dim, st[ndim], lda * nbatch, lda);
-    Bk.st[0] = stage_backward(dif[ipl], p, ipl, f64);
-    set_strides_internal(Bk.in_str, Bk.in_cstr, st[ndim]);
-    set_strides_internal(Bk.out_str, Bk.out_cstr, st[ipl]);
-    // the decision is taken on the layout (pointers are checked again at launch)
-    const bool keep = dry;
-    dry = true;
-    const bool ok = fast_kind(F, f64, f64, f64) == 1 && fast_kind(Bk, f64, f64, f64) == 1;
-    dry = keep;
-    if (!ok) return false;
-    // The spectrum is stored x-tiled for the column passes on either side of
-    // the curl: tiles of w x-columns (one 256-thread CTA), each tile [outer][line][w],
-    // so a CTA writes (forward) and reads (inverse) one contiguous block instead
-    // of rows one plane apart.  Its size is whole tiles (w can exceed the padded
-    // row of a short line, up to 64 columns).
-    const int w = fast_col_tile_width(f64 ? 1 : 0, F.st[0].M, COL_TILE_256);
-    const int ax = p.dim, ob = (ax == 1) ? 2 : 1;
-    const int64_t ntiles = (st[ndim].n[0] + w - 1) / w;
-    int64_t tstr_spec[3];
-    tstr_spec[0] = 1;
-    tstr_spec[ax] = w;
-    tstr_spec[ob] = (int64_t)st[ndim].n[ax] * w;
-    const int64_t tile = (int64_t)st[ndim].n[ob] * st[ndim].n[ax] * w;
-    for (int d = 0; d < 3; ++d) F.out_str[d] = Bk.in_str[d] = tstr_spec[d];
-    F.out_tstr = Bk.in_tstr = tile;
-    F.out_cstr = Bk.in_cstr = ntiles * tile;
-    const size_t need = std::max(state_reals(ndim, nbatch) * es,
-                                 (size_t)(ntiles * tile) * 2 * (size_t)es * (size_t)(lda * nbatch));
-    if (spec_bytes < need) {
-        drop_graphs();
-        if (spec_buf) cudaFree(spec_buf);
-        spec_buf = nullptr;
-        check_cuda(cudaMalloc(&spec_buf, need), "spectrum array");
-        spec_bytes = need;
-    }
-    F.in = buf[(ipl - 1) % 2];
-    F.out = spec_buf;
-    fit_lines(F, es);
-    run_pass(F, f64, f64, f64, "rot_fwd");
-    RotArgs R;
-    memset(&R, 0, sizeof(R));
-    R.data = spec_buf;
-    for (int d = 0; d < 3; ++d) R.n[d] = st[ndim].n[d];
-    for (int d = 0; d < 3; ++d) R.str[d] = tstr_spec[d];
-    R.cstr = ntiles * tile;
-    R.tstr = tile;
-    R.tw = w;
-    R.nbatch = nbatch;
-    R.mult = mult_spec(ROT);
-    const double rbytes = 2.0 * (double)st[ndim].n[0] * st[ndim].n[1] * st[ndim].n[2] * 2 * es * 3 * nbatch +
-                          (double)gfold_n[0] * gfold_n[1] * gfold_n[2] * es;
-    const int k = timed_begin("rot_curl", rbytes);
-    check_cuda(launch_rot_mult(R, f64 ? 1 : 0, stream), "curl launch");
-    timed_end(k);
-    Bk.in = spec_buf;
-    Bk.out = buf[(ipl - 1) % 2];
-    fit_lines(Bk, es);
-    run_pass(Bk, f64, f64, f64, "rot_bwd");
-    return true;
-}
-
 void Solver::do_fused(int type, int nbatch) {
     const bool f64 = (precision == 64);
     const int es = f64 ? 8 : 4;
     const int ipl = ndim - 1;
-    if (type == ROT && rot_split(nbatch)) return;
     {
         // fused: forward ndim-1, multiply, backward ndim-1 (in place on state ndim-1)
         const DirPlan& p = fwd[ipl];
@@ -1560,6 +1509,10 @@ int Solver::slab_peers(int n, void* const* cols, const int* xs, const int64_t* p
         if (xs[j] == own[2] && xs[j + 1] == own[3]) mine = j;
     }
     if (mine < 0 || cols[mine] != xbuf || pitch[mine] != xpitch) return -2;
+    // only the register-DFT column kernel stores to / loads from the owners'
+    // arrays: a y pass that would run elsewhere (other line lengths, fast
+    // kernels off) keeps the exchange steps
+    if (!slab_y_fast()) return -2;
     flb::ColArgs::Peers P{};
     for (int j = 0; j < n; ++j) {
         P.col[j] = cols[j];
@@ -1570,6 +1523,34 @@ int Solver::slab_peers(int n, void* const* cols, const int* xs, const int64_t* p
     P.n = n;
     peers = P;
     return 0;
+}
+
+// Whether the share's y forward and y inverse passes both run the register-DFT
+// column kernel on one component (planned on the host, nothing launched).
+bool Solver::slab_y_fast() {
+    const bool keep = dry;
+    const int keep_dim = slab_dim, keep_lo = slab_lo, keep_hi = slab_hi;
+    dry = true;
+    dry_passes.clear();
+    dry_flags.clear();
+    dry_names.clear();
+    dry_fast.clear();
+    slab_dim = 2;
+    slab_lo = own[0];
+    slab_hi = own[1];
+    fwd_pass(1, nullptr, 1);
+    bwd_pass(1, nullptr, STD, 1);
+    bool ok = dry_fast.size() == 2;
+    for (size_t i = 0; ok && i < dry_fast.size(); ++i) ok = dry_fast[i] == 1 && dry_passes[i].ncomp == 1 && dry_passes[i].axis == 1;
+    dry_passes.clear();
+    dry_flags.clear();
+    dry_names.clear();
+    dry_fast.clear();
+    dry = keep;
+    slab_dim = keep_dim;
+    slab_lo = keep_lo;
+    slab_hi = keep_hi;
+    return ok;
 }
 
 // the array of buffer b seen from plane 0 (integer arithmetic: that base may

@@ -168,19 +168,22 @@ int flups_b200_ipc_close(void* dev_ptr);
 int flups_solve_graph(struct Solver* s, double* field, double* rhs, int nbatch, int type);
 
 /* One solve that allocates no device memory, for callers that cannot call
- * cudaMalloc while they run: code captured into a CUDA graph in the global
- * capture mode, real-time loops that must stay out of the allocator, and
- * frameworks that reserve the device memory for their own pools.  No
- * reference counterpart.  The per-solve scratch (work arrays and twiddle
- * tables) lives in one file-scope device array of 64 MiB held by every GPU
- * that loads the library; solves that need more are refused (return -3).
- * field and rhs must be device pointers, flups_setup must have run (it
- * allocates), and the call only enqueues on the solver's stream (synchronise
- * before reading field).  The first call on a device looks up the array's
- * address (cudaGetSymbolAddress): make it before any stream capture.  All
- * calls share the array, so calls that may overlap on the GPU race; nothing
- * in it has to start at zero.  Returns 0, or a negative code with a message
- * on stderr (-1 not set up, -2 bad arguments, -3 too large, -4 CUDA error). */
+ * cudaMalloc while they run: real-time loops that must stay out of the
+ * allocator (cudaMalloc can synchronise the device and takes driver locks,
+ * so its latency has no bound), and frameworks that reserve the device
+ * memory for their own pools at start-up, after which a cudaMalloc fails.
+ * No counterpart in the reference (its solve allocates nothing per call but
+ * runs on the host).  The per-solve scratch (work arrays and twiddle tables)
+ * lives in one file-scope device array of 64 MiB held by every GPU that
+ * loads the library until the process exits; solves that need more are
+ * refused (return -3).  field and rhs must be device pointers, flups_setup
+ * must have run (it allocates), and the call only enqueues on the solver's
+ * stream (synchronise before reading field).  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress): make it before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents, so calls that may overlap on the GPU race; nothing in it has to
+ * start at zero.  Returns 0, or a negative code with a message on stderr
+ * (-1 not set up, -2 bad arguments, -3 too large, -4 CUDA error). */
 int flups_solve_noalloc(struct Solver* s, double* field, double* rhs, int type);
 
 /* Alternative names of two reference calls:

@@ -107,10 +107,10 @@ def test_fast_fp32_matches_oracle_and_general_engine(name, nglob, lda, bcv, cent
 
 
 @pytest.mark.parametrize("n,odiff,kernel", [(32, 1, LGF_2), (48, 2, HEJ_2), (64, 4, CHAT_2)])
-def test_rot_split_matches_oracle(n, odiff, kernel):
-    """ROT solves whose last direction runs through the register DFTs are split
-    into forward DFT, pointwise curl and Green's multiply, inverse DFT: FP64
-    against the oracle (<= 1e-12), FP32 against the FP64 mode (<= 2e-6)."""
+def test_rot_fused_matches_oracle(n, odiff, kernel):
+    """ROT solves whose last direction runs through the register DFTs do the
+    curl and Green's multiply inside that pass (three components per CTA):
+    FP64 against the oracle (<= 1e-12), FP32 against the FP64 mode (<= 2e-6)."""
     from gpu_helpers import gpu_solve
     nglob = [n] * 3
     bcv = [[[4] * 3, [4] * 3]] * 3

@@ -1,0 +1,127 @@
+"""The kernel instances of the measured workloads, pinned to the oracle on
+cheap grids that select them.
+
+The 512^3 all-unbounded solve runs 512-point half-length r2c / c2r rows
+(1024-point real lines), 1024-point y columns (forward and inverse) and the
+1024-point fused z pass; a 1024-point line is the first whose second
+Stockham stage has radix 32.  Anisotropic grids put one of these line
+lengths in one direction and short lines in the others, so the oracle (FP64
+numpy, the reference's FFTW calls of src/FFTW_plan_dim.cpp:681-716) finishes
+in seconds.  The same is done for the longest lines the register DFTs take
+(4096-point rows, 2048-point columns, 3 x 2^k up to 3072 / 1536), for the
+node-centred DCT-III / DCT-II rows of n = 512 (513 x 257 x 257 workload) and
+for one full 256^3 solve.  Each case also checks, through the host plan
+description, that the passes of the intended length run the register DFTs.
+FP64 <= 1e-12 and FP32 <= 2e-6 relative L2 against the oracle.
+"""
+import numpy as np
+import pytest
+
+from gpu_helpers import from_user, make_solver, oracle_solve, rel_l2, to_user
+from oracle.plans import CELL_CENTER, NODE_CENTER, CHAT_2, LGF_2, LGF_4, HEJ_4
+
+pytestmark = pytest.mark.gpu
+
+UNB3 = [[[4], [4]]] * 3
+EO_PER_UNB = [[[0], [1]], [[3], [3]], [[4], [4]]]
+
+# (name, nglob, bc, centring, kernel, line length M whose passes must run the register DFTs, axis)
+CASES = [
+    ("rows1024_512x32x32", [512, 32, 32], UNB3, CELL_CENTER, LGF_2, 1024, 0),
+    ("cols1024_32x512x32", [32, 512, 32], UNB3, CELL_CENTER, LGF_2, 1024, 1),
+    ("fused1024_32x32x512", [32, 32, 512], UNB3, CELL_CENTER, LGF_2, 1024, 2),
+    ("rows4096_2048x16x16", [2048, 16, 16], UNB3, CELL_CENTER, LGF_2, 4096, 0),
+    ("cols2048_16x1024x16", [16, 1024, 16], UNB3, CELL_CENTER, LGF_2, 2048, 1),
+    ("fused2048_16x16x1024", [16, 16, 1024], UNB3, CELL_CENTER, LGF_2, 2048, 2),
+    ("rows3072_1536x16x16", [1536, 16, 16], UNB3, CELL_CENTER, CHAT_2, 3072, 0),
+    ("cols1536_16x768x16", [16, 768, 16], UNB3, CELL_CENTER, CHAT_2, 1536, 1),
+    ("fused1536_16x16x768", [16, 16, 768], UNB3, CELL_CENTER, CHAT_2, 1536, 2),
+    ("node513_dct_rows_eo_per_unb", [513, 33, 33], EO_PER_UNB, NODE_CENTER, HEJ_4, 1024, 0),
+]
+
+
+def _rhs(nglob, lda=1, seed=17):
+    rng = np.random.default_rng(seed)
+    x = [np.arange(n) / n for n in nglob]
+    X, Y, Z = np.meshgrid(*x, indexing="ij")
+    out = np.zeros((lda,) + tuple(nglob))
+    for c in range(lda):
+        for _ in range(6):
+            cc = rng.uniform(0.2, 0.8, 3)
+            s = rng.uniform(0.03, 0.08)
+            out[c] += rng.uniform(-1, 1) * np.exp(-((X - cc[0]) ** 2 + (Y - cc[1]) ** 2 + (Z - cc[2]) ** 2) / s ** 2)
+        out[c] += 1e-3 * rng.standard_normal(nglob)
+    return out
+
+
+def _grid(nglob, center):
+    fact = 0 if center == CELL_CENTER else 1
+    h = [1.0 / (nglob[0] - fact)] * 3
+    L = [h[d] * (nglob[d] - fact) for d in range(3)]
+    return h, L
+
+
+def _solve(nglob, lda, bcv, center, kernel, precision, rhs, type_=0, odiff=0):
+    h, L = _grid(nglob, center)
+    t, s = make_solver(nglob, lda, bcv, h, L, center, kernel, odiff=odiff, precision=precision)
+    plan = s.plan_json(type_)
+    u = to_user(rhs)
+    out = np.zeros_like(u)
+    s.solve(out, u, type_)
+    assert s.last_error() == 0
+    return from_user(out, lda, nglob), plan
+
+
+_REF = {}
+
+
+def _oracle(name, nglob, lda, bcv, center, kernel, rhs, type_=0, odiff=0):
+    if name not in _REF:
+        h, L = _grid(nglob, center)
+        _REF[name] = oracle_solve(nglob, lda, bcv, h, L, center, kernel, rhs, type_=type_, odiff=odiff)
+    return _REF[name]
+
+
+def _check_fast(plan, M, axis):
+    sel = [p for p in plan["passes"] if p["name"] != "green" and p["axis"] == axis and p["st"][0]["M"] == M]
+    assert sel, f"no pass of {M}-point lines along axis {axis}"
+    assert all(p["fast"] for p in sel), sel
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("name,nglob,bcv,center,kernel,M,axis", CASES, ids=[c[0] for c in CASES])
+def test_kernel_instance_matches_oracle(name, nglob, bcv, center, kernel, M, axis, precision, tol):
+    rhs = _rhs(nglob)
+    got, plan = _solve(nglob, 1, bcv, center, kernel, precision, rhs)
+    _check_fast(plan, M, axis)
+    ref = _oracle(name, nglob, 1, bcv, center, kernel, rhs)
+    assert rel_l2(got, ref) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
+def test_rot_768_point_lines_lgf4(precision, tol):
+    """The ROT solve of the 384^3 vortex-ring workload (LGF_4, spectral curl)
+    on 768-point z lines: 32 x 32 x 384 cells, three components."""
+    nglob = [32, 32, 384]
+    bcv = [[[4] * 3, [4] * 3]] * 3
+    rhs = _rhs(nglob, lda=3, seed=23)
+    got, plan = _solve(nglob, 3, bcv, CELL_CENTER, LGF_4, precision, rhs, type_=1, odiff=1)
+    # the last direction: forward DFT, curl and Green's multiply, inverse DFT in one register-DFT pass
+    fused = [p for p in plan["passes"] if p["name"] == "fused"]
+    assert len(fused) == 1 and fused[0]["fast"] == 1 and fused[0]["st"][0]["M"] == 768, fused
+    ref = _oracle("rot768", nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
+    assert rel_l2(got, ref) <= tol
+
+
+def test_full_256_cube_fp64_matches_oracle():
+    """One full 256^3 all-unbounded FP64 solve (512-point lines in every
+    direction, the instances the graph and slab tests only compare with the
+    library itself) against the oracle."""
+    n = 256
+    nglob = [n] * 3
+    rhs = _rhs(nglob, seed=29)
+    got, plan = _solve(nglob, 1, UNB3, CELL_CENTER, CHAT_2, 64, rhs)
+    for axis in range(3):
+        _check_fast(plan, 2 * n, axis)
+    ref = _oracle("full256", nglob, 1, UNB3, CELL_CENTER, CHAT_2, rhs)
+    assert rel_l2(got, ref) <= 1e-12

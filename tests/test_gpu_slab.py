@@ -92,3 +92,34 @@ def test_slab_refuses_other_problems():
     s = pf.Solver(t, [[pf.BoundaryType.UNB, pf.BoundaryType.UNB]] * 3, [1 / 32] * 3, [1.0] * 3)
     with pytest.raises(ValueError):
         SlabRank(s, 0, 2)
+
+
+def test_slab_peers_refused_without_register_dft_y_passes():
+    """50^3 unbounded has 100-point lines, which the register DFTs do not
+    cover: the y passes run the general line pass, which cannot store into
+    the owners' column arrays, so connecting the peers is refused (-2) and
+    the all-to-all form still equals the one-rank solve."""
+    import torch
+    from flups_b200.slab import SlabRank, solve_local
+    n, world = 50, 2
+    rng = np.random.default_rng(5)
+    rhs = torch.from_numpy(to_user(rng.standard_normal((1, n, n, n)))).cuda()
+    t, s = make_solver([n] * 3, 1, UNB, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, HEJ_2, precision=64)
+    ref = torch.zeros_like(rhs)
+    s.solve(ref, rhs)
+    torch.cuda.synchronize()
+    keep, ranks = [], []
+    for r in range(world):
+        tr, sr = _unset_solver(n, HEJ_2, 64)
+        keep.append((tr, sr))
+        ranks.append(SlabRank(sr, r, world))
+    from flups_b200.slab import _split_table
+    cols = [r.s.slab_columns_ptr() for r in ranks]
+    pitches = [r.columns_shape[2] for r in ranks]
+    for r in ranks:
+        assert r.s.slab_peers(cols, _split_table(r.plan), pitches) == -2
+    rhs_parts = [rhs[0, r.z0:r.z1].contiguous() for r in ranks]
+    out_parts = [torch.full_like(p, float("nan")) for p in rhs_parts]
+    solve_local(ranks, out_parts, rhs_parts)
+    assert torch.equal(torch.cat(out_parts).unsqueeze(0), ref)
+    assert all(sr.last_error() == 0 for _, sr in keep)
