@@ -231,6 +231,7 @@ void flups_b200_set_fast_kernels(Solver* s, int on) { s->use_fast = on != 0; }
 void flups_b200_set_autotune(Solver* s, int on) { s->autotune = on != 0; }
 void flups_b200_set_overlap(Solver* s, int on) { s->overlap = on != 0; }
 void flups_b200_set_prefetch(Solver* s, int on) { s->prefetch = on != 0; }
+void flups_b200_set_xlast(Solver* s, int on) { s->xlast_on = on != 0; }
 void flups_b200_set_col_tile(Solver* s, int tile) { s->force_tile = (tile == 1 || tile == 2) ? tile : 0; }
 int flups_solve_graph(Solver* s, double* field, double* rhs, int nbatch, int type) {
     if (!s) return -1;

@@ -4,8 +4,8 @@
 namespace flb {
 
 cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    if (c2r) return launch_colreal_shape<float, true>(sh, L, a, ncomp, s);
-    return launch_colreal_shape<float, false>(sh, L, a, ncomp, s);
+    if (c2r) return launch_colreal_shape<float, float, true>(sh, L, a, ncomp, s);
+    return launch_colreal_shape<float, float, false>(sh, L, a, ncomp, s);
 }
 
 }  // namespace flb

@@ -91,6 +91,15 @@ cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncom
     return launch_col_f32_m01(mode, sh, L, a, ncomp, s);
 }
 
+bool fast_rowfused_supported(int f64, int L) { return fast_rowfused_len(L, f64); }
+
+cudaError_t launch_fast_rowfused(int f64, int rot, int L, const RowFusedArgs& a, int ncomp, cudaStream_t s) {
+    auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };
+    const int sh = (shape(a.nin) == shape(a.nout)) ? shape(a.nin) : SH_ANY;
+    if (f64) return launch_rowfused_f64(rot, sh, L, a, ncomp, s);
+    return launch_rowfused_f32(rot, sh, L, a, ncomp, s);
+}
+
 bool fast_r2r_supported(int M) {
     switch (M) {
         case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 2048: return true;
@@ -126,6 +135,7 @@ cudaError_t launch_fast_colreal(int f64, int c2r, int L, const ColArgs& a, int n
     // the periodic copy's extra element is stored apart
     const int sh = c2r ? shape(a.period >= 0 ? a.nout - 1 : a.nout) : shape(a.nin > L ? L : a.nin);
     if (f64) return launch_colreal_f64(c2r, sh, L, a, ncomp, s);
+    if (a.real64) return launch_colreal_f32u(c2r, sh, L, a, ncomp, s);
     return launch_colreal_f32(c2r, sh, L, a, ncomp, s);
 }
 

@@ -33,6 +33,8 @@ struct ColArgs {
     double normfact;
     int tile;               // CTA tile: COL_TILE_DEFAULT, COL_TILE_256 or COL_TILE_128 threads
     int period;             // r2c / c2r columns: index that receives a copy of index 0, or -1
+    int real64;             // r2c / c2r columns in FP32: the real side holds doubles (the user's array)
+    int pairs;              // r2c / c2r columns two at a time (aligned pairs: even strides, 16-byte bases)
     Prefetch pf;            // column passes 0 / 1 along a short-stride axis
     // ROT fused pass (mode 3): the curl's wave-number symbols K_{d,c}(i), one
     // table of complex working-precision values per direction d and component
@@ -54,6 +56,27 @@ struct ColArgs {
 };
 
 enum { COL_TILE_DEFAULT = 0, COL_TILE_256 = 1, COL_TILE_128 = 2 };
+
+// The last-direction pass along x (rows contiguous in memory): forward DFT of
+// each row, Green's multiply (STD) or curl and Green's multiply (ROT, three
+// components), inverse DFT, in place.
+struct RowFusedArgs {
+    const void* in;
+    void* out;
+    int n1, n2;                  // rows (i1, i2), i1 < n1 fastest
+    int nin, nout;               // loaded / stored extent along the row (zero beyond nin)
+    int64_t s1, s2, cstr;        // element strides of the rows and of a component
+    const void* tws;             // later-stage twiddle table of the L-point DFT
+    const void* green;           // folded Green's spectrum; x folded at L
+    int64_t g1, g2;              // its strides along i1, i2 (rows of at least L/2 + 4 values)
+    int f1, f2;                  // fold lengths along i1, i2 (0 = none)
+    // ROT: curl symbols (as in ColArgs), the directions of i1 and i2, and the
+    // Nyquist index of every direction (the index whose negation is itself)
+    const void* ksym;
+    int kstr;
+    int ax1, ax2;
+    int nyq[3];
+};
 
 struct RowArgs {
     const void* in;
@@ -145,6 +168,10 @@ __host__ __device__ inline void fast_stage_exponent(int n, int r1, int e, int* q
 // Green's multiply, inverse) or 3 (forward, curl and Green's multiply of
 // groups of three components, inverse)
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+// fused pass along x rows: lengths whose line fits in one warp
+bool fast_rowfused_supported(int f64, int L);
+// rot: three components per row position (curl and Green's multiply), else STD
+cudaError_t launch_fast_rowfused(int f64, int rot, int L, const RowFusedArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 // r2r rows (DCT / DST I-IV) through an M-point complex register DFT
 bool fast_r2r_supported(int M);

@@ -85,8 +85,16 @@ __host__ __device__ constexpr int stage_table_entries(int n, int r1) {
 // ROWS: the lines of a CTA are thread-index-slow (row passes: p fastest),
 // else thread-index-fast (column passes: the TX columns fastest).
 // GTW: the later-stage table is read from global memory (through L1) even
-// when it is small
-template <typename T, int L, int R1, bool ROWS = false, bool GTW = false>
+// when it is small.
+// WSYNC: every line lies inside one warp (ROWS with P dividing 32), so the
+// exchanges synchronise the warp only
+template <bool WSYNC>
+__device__ __forceinline__ void line_sync() {
+    if constexpr (WSYNC) __syncwarp();
+    else __syncthreads();
+}
+
+template <typename T, int L, int R1, bool ROWS = false, bool GTW = false, bool WSYNC = false>
 struct RegFFT {
     using C = typename CT<T>::C;
     static constexpr int P = L / R1;
@@ -110,6 +118,7 @@ struct RegFFT {
     __device__ static __forceinline__ void stages(C* v, C* sm, int p, const C* __restrict__ tws) {
         constexpr int Rs = fast_gcd(L / Ns, R1);
         static_assert(Rs >= 2 && Rs % 2 == 0, "a later stage needs an even radix");
+        static_assert(!WSYNC || (ROWS && 32 % P == 0), "warp-synchronised lines lie inside one warp");
         constexpr int NB = R1 / Rs;  // butterflies per thread
         constexpr int MR = L / Rs;
         C t[R1];
@@ -146,7 +155,7 @@ struct RegFFT {
 #pragma unroll
                 for (int r = 0; r < Rs; ++r) v[b + NB * r] = t[b * Rs + r];
         } else {
-            __syncthreads();
+            line_sync<WSYNC>();
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const int j = p + P * b;
@@ -160,7 +169,7 @@ struct RegFFT {
                     for (int r = 0; r < Rs; ++r) sm[sw(base + r * Ns)] = t[b * Rs + r];
                 }
             }
-            __syncthreads();
+            line_sync<WSYNC>();
             stages<Ns * Rs, INV>(v, sm, p, tws + L);
         }
     }
@@ -173,7 +182,7 @@ struct RegFFT {
         if constexpr (ZIN) dftz<R1>(v);
         else dftr<R1, INV>(v);
         if constexpr (P > 1) {
-            __syncthreads();
+            line_sync<WSYNC>();
             // sw(p R1 + k) = sw(p R1) + k for k < R1 when R1 divides 32
             if constexpr (32 % R1 == 0) {
                 C* d0 = sm + sw(p * R1);
@@ -183,11 +192,16 @@ struct RegFFT {
 #pragma unroll
                 for (int k = 0; k < R1; ++k) sm[sw(p * R1 + k)] = v[k];
             }
-            __syncthreads();
+            line_sync<WSYNC>();
             stages<R1, INV>(v, sm, p, tws);
         }
     }
 };
+
+// two consecutive reals of one type as one vector
+template <typename IT> struct Vec2;
+template <> struct Vec2<float> { using V = float2; };
+template <> struct Vec2<double> { using V = double2; };
 
 // TMA prefetch into L2 of one box of a 4-D tensor map (a hint: no
 // shared memory, no completion to wait for)
@@ -591,12 +605,304 @@ __global__ void __launch_bounds__(3 * TX * (L / R1), FLB_ROT_MINB) col_rot_kerne
     }
 }
 
+// ---------------------------------------------------------------- rows: fused
+// Last-direction pass along x: rows are contiguous, so a row belongs to P
+// consecutive lanes of one warp (P = L / R1 <= 32) and every exchange of its
+// register DFTs synchronises the warp only; warps run independently.  The
+// row's folded Green's values (L/2 + 1, x folded at L) arrive in the line's
+// shared memory through cp.async while the row loads and the forward DFT run.
+// SH: loaded and stored part (SH_HALF: the zero-padded half is neither loaded
+// nor computed, the truncated half neither computed nor stored).
+template <typename T, int L>
+struct RowFusedTile {
+    static constexpr int GP = ((L / 2 + 1) * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);  // Green's values staged per row
+};
+
+// Register budget: 384 threads per SM in FP32 (up to 170 registers; 512,
+// at 128 registers with a few spilled, ran 1.39 against 1.28 ms for the
+// 1024-point rows of a 512^3 solve), 256 in FP64 (up to 255 registers)
+#ifndef FLB_ROWF_WARPS
+#define FLB_ROWF_WARPS 4
+#endif
+template <typename T>
+struct RowFusedOcc {
+    static constexpr int per_sm = sizeof(T) == 8 ? 256 : 384;
+    static constexpr int blocks = per_sm / (FLB_ROWF_WARPS * 32) > 0 ? per_sm / (FLB_ROWF_WARPS * 32) : 1;
+};
+
+template <typename T, int L, int R1, int WARPS, int SH>
+__global__ void __launch_bounds__(WARPS * 32, RowFusedOcc<T>::blocks) row_fused_kernel(const __grid_constant__ RowFusedArgs a) {
+    using F = RegFFT<T, L, R1, true, true, true>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P, LPW = 32 / P, GP = RowFusedTile<T, L>::GP;
+    constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;
+    constexpr int NST = NLD;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int p = lane % P, li = warp * LPW + lane / P;  // line of the CTA
+    const int64_t row = (int64_t)blockIdx.x * (WARPS * LPW) + li;
+    const int comp = blockIdx.y;
+    const bool valid = row < (int64_t)a.n1 * a.n2;
+    const int i1 = valid ? (int)(row % a.n1) : 0, i2 = valid ? (int)(row / a.n1) : 0;
+    C* line = sm + li * F::SC;
+    T* gs = reinterpret_cast<T*>(sm + WARPS * LPW * F::SC) + li * GP;
+    {
+        const T* g = reinterpret_cast<const T*>(a.green) + (int64_t)fold_idx(i1, a.f1) * a.g1 + (int64_t)fold_idx(i2, a.f2) * a.g2;
+        constexpr int PER = 16 / (int)sizeof(T), CH = GP / PER;
+        for (int e = p; e < CH; e += P) cp_async<16>(gs + e * PER, g + e * PER);
+        cp_async_commit();
+    }
+    const C* in = reinterpret_cast<const C*>(a.in) + comp * a.cstr + (int64_t)i1 * a.s1 + (int64_t)i2 * a.s2 + p;
+    C v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        if (r >= NLD) {
+            v[r] = mkc((T)0, (T)0);
+        } else if constexpr (SH != SH_ANY) {
+            v[r] = in[P * r];
+        } else {
+            const bool ok = p + P * r < a.nin;
+            const C u = in[ok ? P * r : 0];
+            v[r] = ok ? u : mkc((T)0, (T)0);
+        }
+    }
+    const C* tws = reinterpret_cast<const C*>(a.tws);
+    F::template fft<SH == SH_HALF, false>(v, line, p, tws);
+    cp_async_wait_all();
+    __syncwarp();
+    // k = p + P r; fold(k) = k for r < R1/2, L - k above; the stored spectrum carries the normalisation
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = cscale(v[r], r < R1 / 2 ? gs[p + P * r] : gs[L - p - P * r]);
+    int zero = 0;
+    asm("" : "+r"(zero));
+    F::template fft<false, true>(v, line, p, tws + zero);
+    if (valid) {
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.cstr + (int64_t)i1 * a.s1 + (int64_t)i2 * a.s2 + p;
+#pragma unroll
+        for (int r = 0; r < NST; ++r) {
+            if (SH != SH_ANY || p + P * r < a.nout) out[P * r] = v[r];
+        }
+    }
+}
+
+// ROT along x rows: warps in triples, warp g of a triple holding component g
+// of LPW row positions; after the forward DFT the three warps of a triple
+// meet at a named barrier (no other warp waits) to read each other's spectra
+// for the curl, as in col_rot_kernel.
+//
+// With x last, z is the real-to-complex direction, and the spectrum kept is
+// kz <= N instead of the reference's kx <= N.  An odd derivative is not
+// Hermitian at a Nyquist index (its symbol there equals that of the negated
+// index), so the two orders would discard different parts of the curl in
+// their final complex-to-real transform.  The row kernel therefore forms the
+// reference's spectrum: the curl with the symbols at +k (P) for 0 < kx < N,
+// the conjugate of the curl at -k (Q = conj of the symbols at -k, which is
+// the symbol at k with its sign flipped except at a Nyquist index) for
+// kx > N, and (P + Q) / 2 at kx = 0 and kx = N (the reference's x
+// complex-to-real keeps the real part there).
+#ifndef FLB_ROWROT_TRIPLES
+#define FLB_ROWROT_TRIPLES 2
+#endif
+template <typename T, int L, int R1, int NT, int SH>
+__global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 0 ? RowFusedOcc<T>::per_sm / (NT * 96) : 1)
+    row_rot_kernel(const __grid_constant__ RowFusedArgs a) {
+    using F = RegFFT<T, L, R1, true, true, true>;
+    using C = typename CT<T>::C;
+    constexpr int P = F::P, LPW = 32 / P, GP = RowFusedTile<T, L>::GP;
+    constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;
+    constexpr int NST = NLD;
+    static_assert(NT >= 1 && NT <= 15, "named barriers 1..15");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tri = warp / 3, g = warp % 3;
+    const int p = lane % P, lw = lane / P;
+    const int64_t row = (int64_t)blockIdx.x * (NT * LPW) + tri * LPW + lw;  // row position
+    const bool valid = row < (int64_t)a.n1 * a.n2;
+    const int i1 = valid ? (int)(row % a.n1) : 0, i2 = valid ? (int)(row / a.n1) : 0;
+    const int comp = 3 * blockIdx.y + g;
+    // lines of the triple: [component][lw]; Green's rows of the triple after all lines
+    auto line_of = [&](int gg) { return sm + ((tri * 3 + gg) * LPW + lw) * F::SC; };
+    C* line = line_of(g);
+    T* gs = reinterpret_cast<T*>(sm + NT * 3 * LPW * F::SC) + (tri * LPW + lw) * GP;
+    if (g == 0) {
+        const T* gr = reinterpret_cast<const T*>(a.green) + (int64_t)fold_idx(i1, a.f1) * a.g1 + (int64_t)fold_idx(i2, a.f2) * a.g2;
+        constexpr int PER = 16 / (int)sizeof(T), CH = GP / PER;
+        for (int e = p; e < CH; e += P) cp_async<16>(gs + e * PER, gr + e * PER);
+        cp_async_commit();
+    }
+    const C* in = reinterpret_cast<const C*>(a.in) + comp * a.cstr + (int64_t)i1 * a.s1 + (int64_t)i2 * a.s2 + p;
+    C v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+        if (r >= NLD) {
+            v[r] = mkc((T)0, (T)0);
+        } else if constexpr (SH != SH_ANY) {
+            v[r] = in[P * r];
+        } else {
+            const bool ok = p + P * r < a.nin;
+            const C u = in[ok ? P * r : 0];
+            v[r] = ok ? u : mkc((T)0, (T)0);
+        }
+    }
+    const C* tws = reinterpret_cast<const C*>(a.tws);
+    F::template fft<SH == SH_HALF, false>(v, line, p, tws);
+    // the curl terms of component g: K_a = K_{g+1, g+2} w_{g+2} - K_b = K_{g+2, g+1} w_{g+1};
+    // x (the line) is direction 0, i1 and i2 are directions a.ax1 and a.ax2
+    const int ga = (g + 2) % 3, gb = (g + 1) % 3;
+    const C* K = reinterpret_cast<const C*>(a.ksym);
+    auto at = [&](int d) { return d == a.ax1 ? i1 : i2; };
+    const C* ktab = nullptr;
+    int vary = 0;
+    C ka = mkc((T)0, (T)0), kb = mkc((T)0, (T)0);
+    // sign of the symbol at the negated index, for the symbols constant along the row
+    T sa = (T)-1, sb = (T)-1;
+    if (gb == 0) {
+        vary = 1;
+        ktab = K + (3 * gb + ga) * a.kstr;
+    } else {
+        ka = K[(3 * gb + ga) * a.kstr + at(gb)];
+        if (at(gb) == a.nyq[gb]) sa = (T)1;
+    }
+    if (ga == 0) {
+        vary = 2;
+        ktab = K + (3 * ga + gb) * a.kstr;
+    } else {
+        kb = K[(3 * ga + gb) * a.kstr + at(ga)];
+        if (at(ga) == a.nyq[ga]) sb = (T)1;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    if (g == 0) cp_async_wait_all();
+    asm volatile("bar.sync %0, 96;" ::"r"(1 + tri) : "memory");
+    {
+        const C* fa = line_of(ga);
+        const C* fb = line_of(gb);
+        auto curl = [&](auto mode) {
+            constexpr int VARY = decltype(mode)::value;
+#pragma unroll
+            for (int r = 0; r < R1; ++r) {
+                const int k = p + P * r;
+                const C A = (VARY == 1) ? __ldg(ktab + k) : ka;
+                const C B = (VARY == 2) ? __ldg(ktab + k) : kb;
+                const C wa = fa[F::sw(k)], wb = fb[F::sw(k)];
+                C u = csub(cmul(wa, A), cmul(wb, B));
+                // kx >= L/2 and kx = 0: the reference's form (see above); the
+                // line's own symbol flips sign at -k except at kx = L/2
+                if (r >= R1 / 2 || (r == 0 && p == 0)) {
+                    const bool edge = (p == 0) && (r == 0 || r == R1 / 2);
+                    const T lsign = (p == 0 && r == R1 / 2) ? (T)1 : (T)-1;
+                    const T qa = (VARY == 1) ? lsign : sa, qb = (VARY == 2) ? lsign : sb;
+                    const C ca = cconj(A), cb = cconj(B);
+                    const C q = csub(cmul(wa, mkc(qa * ca.x, qa * ca.y)), cmul(wb, mkc(qb * cb.x, qb * cb.y)));
+                    u = edge ? mkc((T)0.5 * (u.x + q.x), (T)0.5 * (u.y + q.y)) : q;
+                }
+                v[r] = cscale(u, r < R1 / 2 ? gs[k] : gs[L - k]);
+            }
+        };
+        if (vary == 1) curl(std::integral_constant<int, 1>{});
+        else if (vary == 2) curl(std::integral_constant<int, 2>{});
+        else curl(std::integral_constant<int, 0>{});
+    }
+    // the triple has read every spectrum before the inverse DFT reuses the lines
+    asm volatile("bar.sync %0, 96;" ::"r"(1 + tri) : "memory");
+    int zero = 0;
+    asm("" : "+r"(zero));
+    F::template fft<false, true>(v, line, p, tws + zero);
+    if (valid) {
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.cstr + (int64_t)i1 * a.s1 + (int64_t)i2 * a.s2 + p;
+#pragma unroll
+        for (int r = 0; r < NST; ++r) {
+            if (SH != SH_ANY || p + P * r < a.nout) out[P * r] = v[r];
+        }
+    }
+}
+
+template <typename T, int L, int NT, int SH>
+inline cudaError_t launch_row_rot_t(const RowFusedArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, 2);
+    using F = RegFFT<T, L, R1, true, true, true>;
+    constexpr int LPW = 32 / F::P;
+    constexpr size_t smem = (size_t)NT * LPW * (3 * F::SC * sizeof(typename CT<T>::C) + RowFusedTile<T, L>::GP * sizeof(T));
+    static_assert(smem <= 227 * 1024, "row tile too large");
+    if (ncomp % 3 != 0 || a.g1 < RowFusedTile<T, L>::GP || (reinterpret_cast<uintptr_t>(a.green) & 15) != 0 ||
+        (a.g1 * sizeof(T)) % 16 != 0 || (a.g2 * sizeof(T)) % 16 != 0)
+        return cudaErrorInvalidValue;
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, row_rot_kernel<T, L, R1, NT, SH>, smem); e != cudaSuccess) return e;
+    const int64_t rows = (int64_t)a.n1 * a.n2;
+    dim3 grid((unsigned)((rows + NT * LPW - 1) / (NT * LPW)), ncomp / 3);
+    row_rot_kernel<T, L, R1, NT, SH><<<grid, NT * 96, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// lines of first radix R1 whose P = L / R1 threads fit in one warp
+__host__ __device__ constexpr bool fast_rowfused_len(int L, int f64) {
+    return (L == 48 || L == 64 || L == 96 || L == 128 || L == 192 || L == 256 || L == 384 || L == 512 || L == 768 || L == 1024) &&
+           L / fast_radix1_mode(L, f64, 2) <= 32;
+}
+
+template <typename T, int L, int WARPS, int SH>
+inline cudaError_t launch_row_fused_t(const RowFusedArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, 2);
+    using F = RegFFT<T, L, R1, true, true, true>;
+    constexpr int LPW = 32 / F::P;
+    constexpr size_t smem = (size_t)WARPS * LPW * (F::SC * sizeof(typename CT<T>::C) + RowFusedTile<T, L>::GP * sizeof(T));
+    static_assert(smem <= 227 * 1024, "row tile too large");
+    if (a.g1 < RowFusedTile<T, L>::GP || (reinterpret_cast<uintptr_t>(a.green) & 15) != 0 || (a.g1 * sizeof(T)) % 16 != 0 ||
+        (a.g2 * sizeof(T)) % 16 != 0)
+        return cudaErrorInvalidValue;
+    static std::atomic<unsigned long long> attr{0};
+    if (cudaError_t e = smem_attr_once(attr, row_fused_kernel<T, L, R1, WARPS, SH>, smem); e != cudaSuccess) return e;
+    const int64_t rows = (int64_t)a.n1 * a.n2;
+    dim3 grid((unsigned)((rows + WARPS * LPW - 1) / (WARPS * LPW)), ncomp);
+    row_fused_kernel<T, L, R1, WARPS, SH><<<grid, WARPS * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename T, int SH, bool ROT>
+inline cudaError_t launch_row_fused_len(int L, const RowFusedArgs& a, int ncomp, cudaStream_t s) {
+    constexpr int f64 = sizeof(T) == 8;
+    switch (L) {
+#define FLB_ROWF_CASE(n)                                                                        \
+    case n:                                                                                     \
+        if constexpr (fast_rowfused_len(n, f64)) {                                              \
+            if constexpr (ROT) return launch_row_rot_t<T, n, FLB_ROWROT_TRIPLES, SH>(a, ncomp, s); \
+            else return launch_row_fused_t<T, n, FLB_ROWF_WARPS, SH>(a, ncomp, s);              \
+        }                                                                                       \
+        break;
+        FLB_ROWF_CASE(48)
+        FLB_ROWF_CASE(64)
+        FLB_ROWF_CASE(96)
+        FLB_ROWF_CASE(128)
+        FLB_ROWF_CASE(192)
+        FLB_ROWF_CASE(256)
+        FLB_ROWF_CASE(384)
+        FLB_ROWF_CASE(512)
+        FLB_ROWF_CASE(768)
+        FLB_ROWF_CASE(1024)
+#undef FLB_ROWF_CASE
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename T, bool ROT>
+inline cudaError_t launch_row_fused_shape(int sh, int L, const RowFusedArgs& a, int ncomp, cudaStream_t s) {
+    if (sh == SH_FULL) return launch_row_fused_len<T, SH_FULL, ROT>(L, a, ncomp, s);
+    if (sh == SH_HALF) return launch_row_fused_len<T, SH_HALF, ROT>(L, a, ncomp, s);
+    return launch_row_fused_len<T, SH_ANY, ROT>(L, a, ncomp, s);
+}
+
 // ---------------------------------------------------------------- columns, real side
 // r2c (C2R = false): real column of nin values (zero beyond) -> X[0..L/2];
 // SH: loaded part.  c2r (C2R = true): X[0..L/2] -> real column, the upper half
 // of the spectrum read as conj(X[L-k]) straight from memory (no exchange);
 // SH: stored part.  Im X[0] and Im X[L/2] do not enter a real result.
-template <typename T, int L, int R1, int TX, bool C2R, int SH>
+// RT: type of the real side (the working precision, or the user's doubles
+// when the pass is the first or last of a solve).
+template <typename T, typename RT, int L, int R1, int TX, bool C2R, int SH>
 __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) col_real_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
@@ -612,8 +918,8 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) c
     C v[R1];
     if constexpr (!C2R) {
         constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;
-        const T* in = valid ? reinterpret_cast<const T*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
-                            : reinterpret_cast<const T*>(a.in);
+        const RT* in = valid ? reinterpret_cast<const RT*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+                             : reinterpret_cast<const RT*>(a.in);
         const int ls = valid ? P * (int)a.in_lstr : 0;
 #pragma unroll
         for (int r = 0; r < R1; ++r) {
@@ -621,8 +927,8 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) c
                 v[r] = mkc((T)0, (T)0);
             } else {
                 const bool ok = valid && (SH != SH_ANY || p + P * r < a.nin);
-                const T t = in[ok ? r * ls : 0];
-                v[r] = mkc(ok ? t : (T)0, (T)0);
+                const RT t = in[ok ? r * ls : 0];
+                v[r] = mkc(ok ? (T)t : (T)0, (T)0);
             }
         }
     } else {
@@ -657,13 +963,159 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) c
         if (p == 0 && a.period >= 0) out[(int64_t)a.period * a.out_lstr] = v[0];
     } else {
         constexpr int NST = (SH == SH_HALF) ? R1 / 2 : R1;
-        T* out = reinterpret_cast<T*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        RT* out = reinterpret_cast<RT*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
         const int os = P * (int)a.out_lstr;
 #pragma unroll
         for (int r = 0; r < NST; ++r) {
-            if (SH != SH_ANY || p + P * r < a.nout) out[r * os] = v[r].x;
+            if (SH != SH_ANY || p + P * r < a.nout) out[r * os] = (RT)v[r].x;
         }
-        if (p == 0 && a.period >= 0) out[(int64_t)a.period * a.out_lstr] = v[0].x;
+        if (p == 0 && a.period >= 0) out[(int64_t)a.period * a.out_lstr] = (RT)v[0].x;
+    }
+}
+
+// ---------------------------------------------------------------- columns, real side, in pairs
+// The same transforms for two neighbouring columns (x, x + 1) at once: one
+// complex DFT of z = a + i b.  r2c: A_k = (Z_k + conj Z_{L-k}) / 2 and
+// B_k = (Z_k - conj Z_{L-k}) / 2i, for k <= L/2 (Z_{L-k} from the line in
+// shared memory); c2r: Z_k = A_k + i B_k with A_{L-k} = conj A_k (both halves
+// read straight from memory), one inverse DFT, a = Re z, b = Im z.  Half the
+// arithmetic of one DFT per column, and every global access moves a pair:
+// 16 bytes of the real side (doubles) or of the complex side (FP32).  The
+// host requires the pairs to be aligned (even strides, aligned base); an odd
+// last column is the pair's first half alone.
+template <typename T>
+struct CPair {
+    using C = typename CT<T>::C;
+    __device__ static __forceinline__ void ld(const C* p, C& a, C& b) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 q = *reinterpret_cast<const float4*>(p);
+            a = make_float2(q.x, q.y);
+            b = make_float2(q.z, q.w);
+        } else {
+            a = p[0];
+            b = p[1];
+        }
+    }
+    __device__ static __forceinline__ void st(C* p, C a, C b) {
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+        } else {
+            p[0] = a;
+            p[1] = b;
+        }
+    }
+};
+
+template <typename T, typename RT, int L, int R1, int TXP, bool C2R, int SH>
+__global__ void __launch_bounds__(TXP * (L / R1), (Occ<TXP * (L / R1)>::blocks)) col_real_pair_kernel(const ColArgs a) {
+    using F = RegFFT<T, L, R1>;
+    using C = typename CT<T>::C;
+    using R2 = typename Vec2<RT>::V;
+    constexpr int P = F::P;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int c = threadIdx.x % TXP, p = threadIdx.x / TXP;
+    const int x = 2 * (blockIdx.x * TXP + c);  // first column of the pair
+    const int o = blockIdx.y;
+    const int comp = blockIdx.z;
+    const bool valid = x < a.nx, two = x + 1 < a.nx;
+    const C* tws = stage_twiddles<F>(a.tws, sm + TXP * F::SC);
+    C* line = sm + c * F::SC;
+    C v[R1];
+    const T z = (T)0;
+    if constexpr (!C2R) {
+        constexpr int NLD = (SH == SH_HALF) ? R1 / 2 : R1;
+        const RT* in = valid ? reinterpret_cast<const RT*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x + (int64_t)p * a.in_lstr
+                             : reinterpret_cast<const RT*>(a.in);
+        const int ls = valid ? P * (int)a.in_lstr : 0;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            if (r >= NLD) {
+                v[r] = mkc(z, z);
+            } else {
+                const bool ok = valid && (SH != SH_ANY || p + P * r < a.nin);
+                if (two) {
+                    const R2 t = *reinterpret_cast<const R2*>(in + (ok ? r * ls : 0));
+                    v[r] = ok ? mkc((T)t.x, (T)t.y) : mkc(z, z);
+                } else {
+                    const RT t = in[ok ? r * ls : 0];
+                    v[r] = mkc(ok ? (T)t : z, z);
+                }
+            }
+        }
+        if constexpr (F::TWS) cp_async_wait<0>();
+        F::template fft<SH == SH_HALF, false>(v, line, p, tws);
+        // Z_{L-k} from the line: every thread's spectrum in shared memory
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+        __syncthreads();
+        if (!valid) return;
+        C* out = reinterpret_cast<C*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int os = P * (int)a.out_lstr;
+        auto split = [&](C zk, int k, C& A, C& B) {
+            const C zm = cconj(line[F::sw(k == 0 ? 0 : L - k)]);
+            A = mkc((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y + zm.y));
+            B = mkc((T)0.5 * (zk.y - zm.y), (T)-0.5 * (zk.x - zm.x));  // (Z_k - conj Z_{L-k}) / 2i
+        };
+#pragma unroll
+        for (int r = 0; r <= R1 / 2; ++r) {
+            if (r < R1 / 2 || p == 0) {
+                C A, B;
+                split(v[r], p + P * r, A, B);
+                if (two) CPair<T>::st(out + r * os, A, B);
+                else out[r * os] = A;
+            }
+        }
+        if (p == 0 && a.period >= 0) {
+            C A, B;
+            split(v[0], 0, A, B);
+            C* q = out + (int64_t)a.period * a.out_lstr;
+            if (two) CPair<T>::st(q, A, B);
+            else *q = A;
+        }
+    } else {
+        // Z_k = A_k + i B_k; for k > L/2 from conj A_{L-k}, conj B_{L-k}
+        const C* base = valid ? reinterpret_cast<const C*>(a.in) + comp * a.in_cstr + (int64_t)o * a.in_ostr + x
+                              : reinterpret_cast<const C*>(a.in);
+        const int lstr = valid ? (int)a.in_lstr : 0;
+        const C* lo = base + (int64_t)p * lstr;
+        const C* hi = base + (int64_t)(L - p) * lstr;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            C A, B = mkc(z, z);
+            const C* q = (r < R1 / 2) ? lo + r * P * lstr : hi - r * P * lstr;
+            if (two) CPair<T>::ld(q, A, B);
+            else A = *q;
+            // Im A_0, Im B_0 and Im A_{L/2}, Im B_{L/2} do not enter real results
+            if ((r == 0 || r == R1 / 2) && p == 0) {
+                A.y = z;
+                B.y = z;
+            }
+            if (r >= R1 / 2) {
+                A = cconj(A);
+                B = cconj(B);
+            }
+            v[r] = valid ? mkc(A.x - B.y, A.y + B.x) : mkc(z, z);
+        }
+        if constexpr (F::TWS) cp_async_wait<0>();
+        F::template fft<false, true>(v, line, p, tws);
+        if (!valid) return;
+        constexpr int NST = (SH == SH_HALF) ? R1 / 2 : R1;
+        RT* out = reinterpret_cast<RT*>(a.out) + comp * a.out_cstr + (int64_t)o * a.out_ostr + x + (int64_t)p * a.out_lstr;
+        const int os = P * (int)a.out_lstr;
+#pragma unroll
+        for (int r = 0; r < NST; ++r) {
+            if (SH != SH_ANY || p + P * r < a.nout) {
+                if (two) *reinterpret_cast<R2*>(out + r * os) = R2{(RT)v[r].x, (RT)v[r].y};
+                else out[r * os] = (RT)v[r].x;
+            }
+        }
+        if (p == 0 && a.period >= 0) {
+            RT* q = out + (int64_t)a.period * a.out_lstr;
+            if (two) *reinterpret_cast<R2*>(q) = R2{(RT)v[0].x, (RT)v[0].y};
+            else *q = (RT)v[0].x;
+        }
     }
 }
 
@@ -678,9 +1130,6 @@ struct RowTiles {
 };
 
 // ---------------------------------------------------------------- rows: r2c
-template <typename IT> struct Vec2;
-template <> struct Vec2<float> { using V = float2; };
-template <> struct Vec2<double> { using V = double2; };
 
 // IT: type of the real input (the user's double array, or the working precision);
 // HALF: nin = Lh (the row is zero-padded to twice its length)
@@ -1143,9 +1592,13 @@ cudaError_t launch_col_f32_m2(int sh, int L, const ColArgs& a, int ncomp, cudaSt
 cudaError_t launch_col_f64_m01(int mode, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f64_m2(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f32_m3(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_rowfused_f32(int rot, int sh, int L, const RowFusedArgs& a, int ncomp, cudaStream_t s);
+cudaError_t launch_rowfused_f64(int rot, int sh, int L, const RowFusedArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_col_f64_m3(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_row_units(int f64, int c2r, int xt64, bool half, int L, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
+// FP32 columns whose real side is the user's doubles
+cudaError_t launch_colreal_f32u(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_r2r_units(int f64, int in64, int out64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_dct2_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_dct3_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
@@ -1252,44 +1705,54 @@ inline cudaError_t launch_rot_shape(int sh, int L, const ColArgs& a, int ncomp, 
     return launch_rot_len<T, SH_ANY>(L, a, ncomp, s);
 }
 
-template <typename T, int L, bool C2R, int SH>
+template <typename T, typename RT, int L, bool C2R, int SH>
 inline cudaError_t launch_colreal_t(const ColArgs& a, int ncomp, cudaStream_t s) {
     constexpr int R1 = fast_radix1_of(L, sizeof(T) == 8);
     constexpr int TX = (L == 512 ? 128 : 256) / (L / R1);
     static_assert(TX >= 1, "tile narrower than one column");
     using F = RegFFT<T, L, R1>;
+    if (a.pairs) {
+        // column pairs: the same threads per CTA, each line two columns
+        constexpr int TXP = TX;
+        const size_t smem = (size_t)(TXP * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
+        static std::atomic<unsigned long long> attr{0};
+        if (cudaError_t e = smem_attr_once(attr, col_real_pair_kernel<T, RT, L, R1, TXP, C2R, SH>, smem); e != cudaSuccess) return e;
+        dim3 grid(((a.nx + 1) / 2 + TXP - 1) / TXP, a.nouter, ncomp);
+        col_real_pair_kernel<T, RT, L, R1, TXP, C2R, SH><<<grid, TXP * F::P, smem, s>>>(a);
+        return cudaGetLastError();
+    }
     const size_t smem = (size_t)(TX * F::SC + F::TW_SMEM) * sizeof(typename CT<T>::C);
     static std::atomic<unsigned long long> attr{0};
-    if (cudaError_t e = smem_attr_once(attr, col_real_kernel<T, L, R1, TX, C2R, SH>, smem); e != cudaSuccess) return e;
+    if (cudaError_t e = smem_attr_once(attr, col_real_kernel<T, RT, L, R1, TX, C2R, SH>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nx + TX - 1) / TX, a.nouter, ncomp);
-    col_real_kernel<T, L, R1, TX, C2R, SH><<<grid, TX * F::P, smem, s>>>(a);
+    col_real_kernel<T, RT, L, R1, TX, C2R, SH><<<grid, TX * F::P, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-template <typename T, bool C2R, int SH>
+template <typename T, typename RT, bool C2R, int SH>
 inline cudaError_t launch_colreal_len(int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     switch (L) {
-        case 48: return launch_colreal_t<T, 48, C2R, SH>(a, ncomp, s);
-        case 64: return launch_colreal_t<T, 64, C2R, SH>(a, ncomp, s);
-        case 96: return launch_colreal_t<T, 96, C2R, SH>(a, ncomp, s);
-        case 128: return launch_colreal_t<T, 128, C2R, SH>(a, ncomp, s);
-        case 192: return launch_colreal_t<T, 192, C2R, SH>(a, ncomp, s);
-        case 256: return launch_colreal_t<T, 256, C2R, SH>(a, ncomp, s);
-        case 384: return launch_colreal_t<T, 384, C2R, SH>(a, ncomp, s);
-        case 512: return launch_colreal_t<T, 512, C2R, SH>(a, ncomp, s);
-        case 768: return launch_colreal_t<T, 768, C2R, SH>(a, ncomp, s);
-        case 1024: return launch_colreal_t<T, 1024, C2R, SH>(a, ncomp, s);
-        case 1536: return launch_colreal_t<T, 1536, C2R, SH>(a, ncomp, s);
-        case 2048: return launch_colreal_t<T, 2048, C2R, SH>(a, ncomp, s);
+        case 48: return launch_colreal_t<T, RT, 48, C2R, SH>(a, ncomp, s);
+        case 64: return launch_colreal_t<T, RT, 64, C2R, SH>(a, ncomp, s);
+        case 96: return launch_colreal_t<T, RT, 96, C2R, SH>(a, ncomp, s);
+        case 128: return launch_colreal_t<T, RT, 128, C2R, SH>(a, ncomp, s);
+        case 192: return launch_colreal_t<T, RT, 192, C2R, SH>(a, ncomp, s);
+        case 256: return launch_colreal_t<T, RT, 256, C2R, SH>(a, ncomp, s);
+        case 384: return launch_colreal_t<T, RT, 384, C2R, SH>(a, ncomp, s);
+        case 512: return launch_colreal_t<T, RT, 512, C2R, SH>(a, ncomp, s);
+        case 768: return launch_colreal_t<T, RT, 768, C2R, SH>(a, ncomp, s);
+        case 1024: return launch_colreal_t<T, RT, 1024, C2R, SH>(a, ncomp, s);
+        case 1536: return launch_colreal_t<T, RT, 1536, C2R, SH>(a, ncomp, s);
+        case 2048: return launch_colreal_t<T, RT, 2048, C2R, SH>(a, ncomp, s);
     }
     return cudaErrorInvalidValue;
 }
 
-template <typename T, bool C2R>
+template <typename T, typename RT, bool C2R>
 inline cudaError_t launch_colreal_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
-    if (sh == SH_FULL) return launch_colreal_len<T, C2R, SH_FULL>(L, a, ncomp, s);
-    if (sh == SH_HALF) return launch_colreal_len<T, C2R, SH_HALF>(L, a, ncomp, s);
-    return launch_colreal_len<T, C2R, SH_ANY>(L, a, ncomp, s);
+    if (sh == SH_FULL) return launch_colreal_len<T, RT, C2R, SH_FULL>(L, a, ncomp, s);
+    if (sh == SH_HALF) return launch_colreal_len<T, RT, C2R, SH_HALF>(L, a, ncomp, s);
+    return launch_colreal_len<T, RT, C2R, SH_ANY>(L, a, ncomp, s);
 }
 
 template <typename T, int MODE>

@@ -198,10 +198,12 @@ struct Solver {
     const void* twiddle_plain(int L, bool f64);   // W_L^q, q < L
     // later-stage twiddles of an n-point register DFT with first radix r1 (0: the default of the precision)
     const void* stage_table(int n, bool f64, int r1 = 0);
-    int fast_kind(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64) const;  // 0 none, 1 column, 2 row
+    // 0 none, 1 column c2c, 2 row r2c/c2r, 3 column r2c/c2r, 4 row r2r, 5 fused row
+    int fast_kind(const flb::PassArgs& A, bool f64, bool in_f64, bool out_f64) const;
     // arguments of a fast launch, all but the twiddle tables; mode of a column pass
     void fast_args(const flb::PassArgs& A, int kind, bool in_f64, bool out_f64, flb::ColArgs& c, flb::RowArgs& r, int& mode) const;
     void launch_fast(const flb::PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64);
+    void rowfused_args(const flb::PassArgs& A, flb::RowFusedArgs& f) const;
     void ensure_buffers(int nbatch);
     flb::LineStage stage_forward(const flb::DirPlan& p, int ip, bool f64);
     flb::LineStage stage_backward(const flb::DirPlan& p, const flb::DirPlan& pf, int ip, bool f64);
@@ -209,6 +211,7 @@ struct Solver {
     void set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s, bool pad = true) const;
     int64_t row_pitch(const ArrState& s) const;             // x extent in memory (128-byte multiple)
     size_t state_reals(int k, int nbatch) const;            // reals held by state k for nbatch right-hand sides
+    size_t work_reals(int b, int nbatch) const;             // reals of work array b (both pass orders)
     void set_strides_user(int64_t str[3], int64_t& cstr) const;
     void fit_lines(flb::PassArgs& A, int elem_bytes) const;
     flb::MultSpec mult_spec(int type) const;
@@ -228,6 +231,26 @@ struct Solver {
     void* ksym = nullptr;
     int kstr = 0;
     void build_ksym();
+    // x-last order of an all-unbounded 3-D problem: z (r2c), y, x, so that the
+    // last direction (forward DFT, multiply, inverse DFT) runs along
+    // contiguous rows, one warp per row.  Solves of device arrays use it; the
+    // reference's order (fwd/bwd/grn/dif) stays the public one (plan tables,
+    // advanced API, host-array and z-slab solves).  swap_order() exchanges
+    // the two sets for the duration of a solve; the folded Green's spectrum
+    // is the same array in both orders.
+    bool has_xlast = false;
+    bool xlast_on = true;                 // flups_b200_set_xlast
+    bool xlast_active = false;
+    flb::DirPlan xfwd[3], xbwd[3], xdif[3];
+    ArrState xst[4];
+    int xgfold_M[3] = {0, 0, 0};
+    void* xksym = nullptr;
+    int xkstr = 0;
+    bool xlast_fast[2] = {false, false};  // STD, ROT: every pass of the x-last order is a register-DFT kernel
+    void build_xlast();
+    void swap_order();
+    void plan_xlast();
+    bool xlast_ok(int type) const;
     void collect_timing();
     void check_cuda(cudaError_t e, const char* what);
     void do_fft_forward(const double* user_in, int nbatch);

@@ -158,6 +158,8 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             slot_for(A.st[0].M, fast_radix1_mode(A.st[0].M, f64 ? 1 : 0, A.fused ? 2 : 0));
         } else if (kinds[i] == 3) {
             slot_for(A.st[0].M, r1_of(A.st[0].M));
+        } else if (kinds[i] == 5) {
+            slot_for(A.st[0].M, fast_radix1_mode(A.st[0].M, f64 ? 1 : 0, 2));
         } else if (kinds[i] == 4) {
             const LineSpec& sp = A.st[0].spec[0];
             slot_for(2 * A.st[0].M, 0);
@@ -199,6 +201,12 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             if (kinds[i] == 0) {
                 for (int sg = 0; sg <= A.fused; ++sg) A.st[sg].tw = tw_of(2 * A.st[sg].M, 0);
                 if (go) e = launch_line_pass(A, f64 ? 1 : 0, in64 ? 1 : 0, out64 ? 1 : 0, st);
+            } else if (kinds[i] == 5) {
+                RowFusedArgs f;
+                s->rowfused_args(A, f);
+                const int L = A.st[0].M;
+                f.tws = tw_of(L, fast_radix1_mode(L, f64 ? 1 : 0, 2));
+                if (go) e = launch_fast_rowfused(f64 ? 1 : 0, A.mult.mode == 2, L, f, A.ncomp, st);
             } else {
                 const int L = A.st[0].M;
                 ColArgs c;

@@ -137,6 +137,92 @@ Solver::Solver(Topology* t, FLUPS_BoundaryType* bcin[3][2], const double hin[3],
         normfact *= fwd[ip].normfact;
         volfact *= fwd[ip].volfact;
     }
+    build_xlast();
+}
+
+// The x-last plans of an all-unbounded 3-D problem (see host.hpp): the same
+// per-direction tables (FFTW_plan_dim_{cell,node}.cpp) initialised in the
+// order z, y, x, so z becomes the real-to-complex direction.
+void Solver::build_xlast() {
+    if (ndim != 3) return;
+    for (int ip = 0; ip < 3; ++ip)
+        if (fwd[ip].type != UNBUNB) return;
+    const int order[3] = {2, 1, 0};
+    for (int k = 0; k < 3; ++k) {
+        const int d = order[k];
+        xfwd[k] = DirPlan(lda, d, h, L, bc[d][0], bc[d][1], FLUPS_FORWARD, false, center);
+        xbwd[k] = DirPlan(lda, d, h, L, bc[d][0], bc[d][1], FLUPS_BACKWARD, false, center);
+        if (have_diff) {
+            int l[3], r[3];
+            for (int c = 0; c < lda; ++c) {
+                auto sw = [](int b) { return b == EVEN ? ODD : (b == ODD ? EVEN : b); };
+                l[c] = sw(bc[d][0][c]);
+                r[c] = sw(bc[d][1][c]);
+            }
+            xdif[k] = DirPlan(lda, d, h, L, l, r, FLUPS_BACKWARD, false, center);
+        }
+    }
+    dry_run(xfwd);
+    dry_run(xbwd);
+    if (have_diff) dry_run(xdif);
+    xst[0] = st[0];
+    for (int ip = 0; ip < ndim; ++ip) {
+        xst[ip + 1] = xst[ip];
+        xst[ip + 1].n[xfwd[ip].dim] = xfwd[ip].n_out;
+        xst[ip + 1].cplx = xst[ip].cplx || xfwd[ip].isr2c;
+    }
+    has_xlast = true;
+}
+
+void Solver::swap_order() {
+    for (int k = 0; k < 3; ++k) {
+        std::swap(fwd[k], xfwd[k]);
+        std::swap(bwd[k], xbwd[k]);
+        std::swap(dif[k], xdif[k]);
+        std::swap(gfold_M[k], xgfold_M[k]);
+    }
+    for (int k = 0; k < 4; ++k) std::swap(st[k], xst[k]);
+    std::swap(ksym, xksym);
+    std::swap(kstr, xkstr);
+    xlast_active = !xlast_active;
+}
+
+// The x-last order runs when every pass of it has a register-DFT kernel and
+// the fused pass is the row kernel (planned on the host at set-up, per
+// solver type).
+bool Solver::xlast_ok(int type) const {
+    if (!has_xlast || !xlast_on || !use_fast || owned() || slab_dim >= 0 || xlast_active) return false;
+    return xlast_fast[type == ROT ? 1 : 0];
+}
+
+void Solver::plan_xlast() {
+    xlast_fast[0] = xlast_fast[1] = false;
+    if (!has_xlast) return;
+    for (int t = 0; t < 2; ++t) {
+        const int type = t ? ROT : STD;
+        if (type == ROT && (lda != 3 || !have_diff)) continue;
+        swap_order();
+        const bool keep = dry;
+        dry = true;
+        dry_passes.clear();
+        dry_flags.clear();
+        dry_names.clear();
+        dry_fast.clear();
+        do_fft_forward(nullptr, 1);
+        do_fft_backward_fused(nullptr, type, 1);
+        bool ok = !dry_fast.empty();
+        for (size_t i = 0; i < dry_fast.size(); ++i) {
+            if (dry_fast[i] == 0) ok = false;
+            if (dry_passes[i].fused && dry_fast[i] != 5) ok = false;
+        }
+        dry_passes.clear();
+        dry_flags.clear();
+        dry_names.clear();
+        dry_fast.clear();
+        dry = keep;
+        swap_order();
+        xlast_fast[t] = ok;
+    }
 }
 
 void Solver::dry_run(DirPlan p[3]) {
@@ -179,7 +265,9 @@ Solver::~Solver() {
     for (auto& kv : twiddles) cudaFree(kv.second);
     if (stage_in) cudaFree(stage_in);
     if (stage_out) cudaFree(stage_out);
+    if (xlast_active) swap_order();
     if (ksym) cudaFree(ksym);
+    if (xksym) cudaFree(xksym);
     if (h2d_stream) {
         for (int k = 0; k < kSlabs; ++k) {
             cudaEventDestroy(ev_in[k]);
@@ -334,6 +422,23 @@ size_t Solver::state_reals(int k, int nbatch) const {
     return (size_t)row_pitch(st[k]) * st[k].n[1] * st[k].n[2] * (st[k].cplx ? 2 : 1) * lda * nbatch;
 }
 
+// reals of work array b (0: states 1, 3, ...; 1: states 2, ...) for nbatch
+// right-hand sides: the larger of the two pass orders when both exist
+size_t Solver::work_reals(int b, int nbatch) const {
+    size_t need = 0;
+    for (int k = 1; k < ndim; ++k) {
+        if ((k - 1) % 2 != b) continue;
+        size_t r = state_reals(k, nbatch);
+        if (owned()) r = r / (size_t)st[k].n[2] * (size_t)(own[1] - own[0]);
+        need = std::max(need, r);
+        if (has_xlast && !owned()) {
+            const ArrState& X = xst[k];
+            need = std::max(need, (size_t)row_pitch(X) * X.n[1] * X.n[2] * (X.cplx ? 2 : 1) * lda * nbatch);
+        }
+    }
+    return need;
+}
+
 void Solver::set_strides_internal(int64_t str[3], int64_t& cstr, const ArrState& s, bool pad) const {
     const int64_t px = pad ? row_pitch(s) : s.n[0];
     str[0] = 1;
@@ -423,7 +528,8 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
     if (!use_fast) return 0;
     // components together: only the fused ROT pass (groups of three components)
     const bool rot = A.fused && A.mult.mode == 2;
-    if (A.comps_together && !(rot && A.lda == 3 && A.ncomp % 3 == 0 && ksym)) return 0;
+    // (the curl tables exist once set up; host-only planning assumes them)
+    if (A.comps_together && !(rot && A.lda == 3 && A.ncomp % 3 == 0 && (ksym || dry))) return 0;
     if (rot && !A.comps_together) return 0;
     if (A.n_b > 65535 || A.ncomp > 65535) return 0;  // grid y / z limits of the fast launches
     // vector loads/stores of complex (or real pairs) need their natural alignment
@@ -439,14 +545,19 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
             const LineSpec& sp0 = S0.spec[0];
             for (int c = 0; c < A.lda; ++c) {
                 const LineSpec& sp = S0.spec[c];
+                // (nfftw only matters to the periodic copy)
                 if (sp.kind != k0 || sp.n_in != sp0.n_in || sp.fi != 0 || sp.fo != 0 || sp.postpro != sp0.postpro ||
-                    sp.nfftw != sp0.nfftw)
+                    (sp0.postpro == PP_ENFORCE_PERIOD && sp.nfftw != sp0.nfftw))
                     return 0;
             }
             if (sp0.postpro != PP_NONE && sp0.postpro != PP_ENFORCE_PERIOD) return 0;
             const int extra = (sp0.postpro == PP_ENFORCE_PERIOD) ? 1 : 0;
             if (S0.fieldstart != 0 || S0.store_off != 0) return 0;
-            if (!fast_col_supported(L) || in_f64 != f64 || out_f64 != f64) return 0;
+            if (!fast_col_supported(L)) return 0;
+            // the complex side is in the working precision; the real side is too, or
+            // it is the user's doubles (first or last pass of an FP32 solve)
+            if ((k0 == LK_R2C ? out_f64 : in_f64) != f64) return 0;
+            if (f64 && (k0 == LK_R2C ? !in_f64 : !out_f64)) return 0;
             if (A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
             if ((int64_t)(L + 1) * A.in_str[A.axis] >= (int64_t)INT32_MAX || (int64_t)(L + 1) * A.out_str[A.axis] >= (int64_t)INT32_MAX)
                 return 0;
@@ -502,7 +613,21 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
         if (!A.fused && S0.n_o != L) return 0;
         return 1;
     }
-    if (A.fused) return 0;
+    if (A.fused) {
+        // the last direction along x: the fused row pass (one warp per row)
+        if (k0 != LK_C2C || !S0.in_cplx || !S0.out_cplx || in_f64 != f64 || out_f64 != f64) return 0;
+        const int L = S0.M;
+        if (A.st[1].spec[0].kind != LK_C2C || A.st[1].M != L || (A.mult.mode != 1 && !rot)) return 0;
+        if (!fast_rowfused_supported(f64 ? 1 : 0, L) || A.n_src > L || A.st[1].n_store > L) return 0;
+        if (A.in_str[0] != 1 || A.out_str[0] != 1 || A.in != A.out) return 0;
+        for (int d = 0; d < 3; ++d)
+            if (A.in_str[d] != A.out_str[d]) return 0;
+        if (A.mult.gfold[0] != L || A.mult.gstr[0] != 1 || A.mult.gstr[1] < L / 2 + 4) return 0;
+        const int64_t es = f64 ? 8 : 4;
+        if ((A.mult.gstr[1] * es) % 16 != 0 || (A.mult.gstr[2] * es) % 16 != 0) return 0;
+        if (!dry && (reinterpret_cast<uintptr_t>(A.mult.green) & 15) != 0) return 0;
+        return 5;
+    }
     const int L = S0.M;
     if (!fast_row_supported(L) || A.in_str[0] != 1 || A.out_str[0] != 1) return 0;
     auto even = [](int64_t v) { return (v % 2) == 0; };
@@ -535,6 +660,15 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
         c.nin = A.n_src;
         c.nout = A.st[A.fused ? 1 : 0].n_store;
         c.period = (kind == 3 && A.st[0].spec[0].postpro == PP_ENFORCE_PERIOD) ? A.st[0].spec[0].nfftw : -1;
+        if (kind == 3) {
+            c.real64 = (S0.spec[0].kind == LK_R2C) ? (in_f64 && !out_f64) : (out_f64 && !in_f64);
+            // neighbouring columns two at a time when every pair is aligned
+            auto even = [](int64_t v) { return (v % 2) == 0; };
+            const bool strides = even(A.in_str[1]) && even(A.in_str[2]) && even(A.in_cstr) && even(A.out_str[1]) &&
+                                 even(A.out_str[2]) && even(A.out_cstr);
+            const bool bases = dry || ((reinterpret_cast<uintptr_t>(A.in) & 15) == 0 && (reinterpret_cast<uintptr_t>(A.out) & 15) == 0);
+            c.pairs = (strides && bases) ? 1 : 0;
+        }
         c.in_lstr = A.in_str[A.axis];
         c.in_ostr = A.in_str[b];
         c.in_cstr = A.in_cstr;
@@ -582,8 +716,46 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
     r.out_f64 = out_f64;
 }
 
+// arguments of the fused row pass (kind 5): rows (y, z) of the x-fastest array
+void Solver::rowfused_args(const PassArgs& A, RowFusedArgs& f) const {
+    memset(&f, 0, sizeof(f));
+    f.in = A.in;
+    f.out = A.out;
+    f.n1 = A.n_a;
+    f.n2 = A.n_b;
+    f.nin = A.n_src;
+    f.nout = A.st[1].n_store;
+    f.s1 = A.in_str[1];
+    f.s2 = A.in_str[2];
+    f.cstr = A.in_cstr;
+    f.green = A.mult.green;
+    f.g1 = A.mult.gstr[1];
+    f.g2 = A.mult.gstr[2];
+    f.f1 = A.mult.gfold[1];
+    f.f2 = A.mult.gfold[2];
+    if (A.mult.mode == 2) {
+        f.ksym = ksym;
+        f.kstr = kstr;
+        f.ax1 = 1;
+        f.ax2 = 2;
+        // the Nyquist index of each direction: half its DFT length
+        for (int ip = 0; ip < ndim; ++ip) {
+            const DirPlan& p = fwd[ip];
+            f.nyq[p.dim] = (p.type == PERPER || p.type == UNBUNB) ? (p.isr2c ? p.n_out - 1 : p.n_in[0] / 2) : -1;
+        }
+        for (int d = ndim; d < 3; ++d) f.nyq[fwd[d].dim] = -1;
+    }
+}
+
 void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, bool out_f64) {
     const int L = A.st[0].M;
+    if (kind == 5) {
+        RowFusedArgs f;
+        rowfused_args(A, f);
+        f.tws = stage_table(L, f64, fast_radix1_mode(L, f64 ? 1 : 0, 2));
+        check_cuda(launch_fast_rowfused(f64 ? 1 : 0, A.mult.mode == 2, L, f, A.ncomp, stream), "fused row launch");
+        return;
+    }
     ColArgs c;
     RowArgs r;
     int mode = 0;
@@ -996,6 +1168,19 @@ void Solver::compute_green() {
     }
     for (int d = 0; d < 3; ++d)
         FLB_CHECK(spec_n[d] == st[ndim].n[d], "Topo of Green has to be the same as Topo of field");
+    if (has_xlast) {
+        // the x-last order folds its complex-to-complex directions the same
+        // way; its folded extents must be those of this array (they are for
+        // every all-unbounded problem: 2N-point lines fold to N + 1 values,
+        // the N + 1 of the real-to-complex direction need no fold)
+        for (int d = 0; d < 3; ++d) xgfold_M[d] = 0;
+        for (int ip = 0; ip < ndim; ++ip) {
+            const DirPlan& p = xfwd[ip];
+            const int fn = (p.type == UNBUNB && !p.isr2c) ? p.n_in[0] / 2 + 1 : xst[ndim].n[p.dim];
+            if (p.type == UNBUNB && !p.isr2c) xgfold_M[p.dim] = p.n_in[0];
+            if (fn != gfold_n[p.dim]) has_xlast = false;
+        }
+    }
     const bool f64 = (precision == 64);
     const int64_t gq = f64 ? 16 : 32;  // rows of the folded spectrum on 128-byte boundaries
     gstr[0] = 1;
@@ -1057,6 +1242,7 @@ void Solver::setup() {
     compute_green();
     if (owned()) slice_green();
     build_ksym();
+    plan_xlast();
     ensure_buffers(1);
     is_setup = true;
 }
@@ -1067,6 +1253,12 @@ void Solver::setup() {
 // pointwise multiply.
 void Solver::build_ksym() {
     if (!have_diff || lda != 3 || dry || ksym) return;
+    if (has_xlast && !xlast_active) {
+        // the x-last order's tables first (its spectral extents and symmetries)
+        swap_order();
+        build_ksym();
+        swap_order();
+    }
     const MultSpec G = mult_spec(ROT);
     int n[3];
     kstr = 1;
@@ -1114,13 +1306,7 @@ void Solver::ensure_buffers(int nbatch) {
         if (!xbuf) check_cuda(cudaMalloc(&xbuf, xneed * es), "column work buffer");
     }
     for (int b = 0; b < 2; ++b) {
-        size_t need = 0;
-        for (int k = 1; k < ndim; ++k) {
-            if ((k - 1) % 2 != b) continue;
-            size_t r = state_reals(k, nbatch);
-            if (owned()) r = r / (size_t)st[k].n[2] * (size_t)(own[1] - own[0]);
-            need = std::max(need, r);
-        }
+        const size_t need = work_reals(b, nbatch);
         if (need > buf_elems[b]) {
             drop_graphs();  // captured solves point at the old arrays
             if (buf[b]) cudaFree(buf[b]);
@@ -1140,20 +1326,12 @@ void Solver::drop_graphs() {
 size_t Solver::device_bytes(int nbatch) const {
     const size_t es = (precision == 64) ? 8 : 4;
     size_t total = 0;
-    for (int b = 0; b < 2; ++b) {
-        size_t need = 0;
-        for (int k = 1; k < ndim; ++k) {
-            if ((k - 1) % 2 != b) continue;
-            size_t r = state_reals(k, nbatch);
-            if (owned()) r = r / (size_t)st[k].n[2] * (size_t)(own[1] - own[0]);
-            need = std::max(need, r);
-        }
-        total += need * es;
-    }
+    for (int b = 0; b < 2; ++b) total += work_reals(b, nbatch) * es;
     if (owned()) total += (size_t)xpitch * st[ndim - 1].n[1] * st[ndim - 1].n[2] * 2 * es;
     // (a share holds its columns of the Green's spectrum: gstr describes that array after set-up)
     total += (size_t)gstr[2] * gfold_n[2] * es;
     if (ksym) total += (size_t)9 * kstr * 2 * es;
+    if (xksym) total += (size_t)9 * xkstr * 2 * es;
     return total;
 }
 
@@ -1352,8 +1530,11 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     if (dev_in && dev_out && overlap_ok(type)) {
         solve_overlap(din, dout, type, nbatch);
     } else {
+        const bool xl = xlast_ok(type);
+        if (xl) swap_order();
         do_fft_forward(din, nbatch);
         do_fft_backward_fused(dout, type, nbatch);
+        if (xl) swap_order();
     }
     collect_timing();
     if (!dev_out) {
@@ -1908,8 +2089,13 @@ std::string Solver::plan_json(int type, int nbatch) {
     dry_names.clear();
     dry_fast.clear();
     compute_green();
+    plan_xlast();
+    // the passes of a solve of device arrays (the x-last order where it applies)
+    const bool xl = xlast_ok(type);
+    if (xl) swap_order();
     do_fft_forward(nullptr, nbatch);
     do_fft_backward_fused(nullptr, type, nbatch);
+    if (xl) swap_order();
     dry = false;
     for (size_t i = 0; i < dry_passes.size(); ++i) {
         const PassArgs& A = dry_passes[i];
@@ -1937,6 +2123,8 @@ std::string Solver::plan_json(int type, int nbatch) {
         }
         o += "]}";
     }
-    o += "]}";
+    o += "],\"xlast\":";
+    o += xl ? "1" : "0";
+    o += "}";
     return o;
 }

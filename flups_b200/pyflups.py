@@ -116,6 +116,7 @@ def load_library(path=None):
         "flups_b200_set_col_tile": (None, [vp, c_int]),
         "flups_b200_set_overlap": (None, [vp, c_int]),
         "flups_b200_set_prefetch": (None, [vp, c_int]),
+        "flups_b200_set_xlast": (None, [vp, c_int]),
         "flups_b200_slab_info": (c_int, [vp, POINTER(ctypes.c_int64)]),
         "flups_b200_slab_own": (c_int, [vp, c_int, c_int, c_int, c_int]),
         "flups_b200_slab_planes": (vp, [vp]),
@@ -194,6 +195,7 @@ class Topology:
     def axis(self):
         return _lib.flups_topo_get_axis(self._ptr)
 
+    @property
     def is_complex(self):
         return bool(_lib.flups_topo_get_isComplex(self._ptr))
 
@@ -214,9 +216,11 @@ class Topology:
         _lib.flups_topo_get_istartGlob(self._ptr, a)
         return np.array(a[:])
 
+    @property
     def locsize(self):
         return _lib.flups_topo_get_locsize(self._ptr)
 
+    @property
     def memsize(self):
         return _lib.flups_topo_get_memsize(self._ptr)
 
@@ -295,7 +299,7 @@ class Solver:
         as a numpy array of doubles, sized for both inner layouts."""
         ptr = _lib.flups_get_innerBuffer(self._solver)
         topo_s = self.get_inner_topo_spectral()
-        n = max(topo_s.memsize(), self._topology.memsize())
+        n = max(topo_s.memsize, self._topology.memsize)
         return np.ctypeslib.as_array((ctypes.c_double * n).from_address(ptr))
 
     def get_inner_topo_physical(self):
@@ -323,6 +327,10 @@ class Solver:
     def set_prefetch(self, on):
         """L2 prefetch of the next blocks' input in the row / column passes (default on)."""
         _lib.flups_b200_set_prefetch(self._solver, int(bool(on)))
+
+    def set_xlast(self, on):
+        """Pass order of all-unbounded 3-D device-array solves: x last (default) or the reference's x first."""
+        _lib.flups_b200_set_xlast(self._solver, int(bool(on)))
 
     # ---- one rank's share of a z-slab decomposed solve (flups_b200/slab.py drives it)
     def slab_info(self):

@@ -35,11 +35,25 @@ def make_solver(nglob, lda, bcv, h, L, center, kernel, odiff=0, precision=64, al
     return t, s
 
 
-def gpu_solve(nglob, lda, bcv, h, L, center, kernel, rhs, type_=0, odiff=0, precision=64, alpha=2.0):
+def gpu_solve(nglob, lda, bcv, h, L, center, kernel, rhs, type_=0, odiff=0, precision=64, alpha=2.0, device=False,
+              xlast=True):
+    """One solve through the C ABI.  device=False passes host (numpy) arrays,
+    which 3-D problems solve in the reference's pass order with slab-streamed
+    copies; device=True passes CUDA arrays (the x-last order of all-unbounded
+    problems unless xlast=False)."""
     t, s = make_solver(nglob, lda, bcv, h, L, center, kernel, odiff, precision, alpha)
+    s.set_xlast(xlast)
     u = to_user(rhs)
-    out = np.zeros_like(u)
-    s.solve(out, u, type_)
+    if device:
+        import torch
+        du = torch.from_numpy(u).cuda()
+        dout = torch.zeros_like(du)
+        s.solve(dout, du, type_)
+        torch.cuda.synchronize()
+        out = dout.cpu().numpy()
+    else:
+        out = np.zeros_like(u)
+        s.solve(out, u, type_)
     err = s.last_error()
     del s, t
     assert err == 0, f"CUDA error {err}"

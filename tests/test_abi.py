@@ -47,10 +47,10 @@ def test_topology_layout_math():
     t = pf.Topology(0, 3, [17, 9, 5])
     assert [t.get_nglob(d) for d in range(3)] == [17, 9, 5]
     assert [t.get_nmem(d) for d in range(3)] == [17, 9, 5]  # 8-byte alignment: no padding for doubles
-    assert t.memsize() == 17 * 9 * 5 * 3
+    assert t.memsize == 17 * 9 * 5 * 3
     t2 = pf.Topology(1, 1, [16, 16, 16], is_complex=True, alignment=64)
     # 16 complex doubles = 256 bytes along the axis: already a multiple of 64
-    assert t2.get_nmem(1) == 16 and t2.is_complex()
+    assert t2.get_nmem(1) == 16 and t2.is_complex
     t3 = pf.Topology(0, 1, [17, 8, 8], alignment=64)
     assert t3.get_nmem(0) == 24  # padded to 64 bytes (src/Topology.cpp:81-98)
 

@@ -83,7 +83,7 @@ def test_spectral_filter_like_the_sample():
     ax0 = ts.axis
     nmem = [ts.get_nmem(d) for d in range(3)]
     nloc = [ts.get_nloc(d) for d in range(3)]
-    assert ts.is_complex()
+    assert ts.is_complex
 
     def sym(i, d):
         if ss[d] == 0.0 or i <= ss[d]:

@@ -122,3 +122,49 @@ def test_rot_fused_matches_oracle(n, odiff, kernel):
     assert rel_l2(got, ref) <= 1e-12
     got32 = gpu_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff, precision=32)
     assert rel_l2(got32, got) <= 2e-6
+
+
+XLAST_CASES = [
+    ("unb64", [64] * 3, NODE_CENTER, CHAT_2),
+    ("unb_aniso", [128, 64, 32], CELL_CENTER, LGF_2),
+    ("unb96_r3", [96, 48, 48], CELL_CENTER, HEJ_2),
+    ("unb_node65", [65, 33, 33], NODE_CENTER, HEJ_4),
+]
+
+
+@pytest.mark.parametrize("name,nglob,center,kernel", XLAST_CASES, ids=[c[0] for c in XLAST_CASES])
+def test_xlast_order_matches_oracle_and_reference_order(name, nglob, center, kernel):
+    """All-unbounded solves of device arrays in the x-last order (z r2c
+    columns of the user's doubles, y columns, fused x rows) against the oracle
+    and against the reference's order on the same device arrays: FP64 within
+    1e-12 of both, FP32 within 2e-6."""
+    from gpu_helpers import gpu_solve
+    n0 = nglob[0] - (0 if center == CELL_CENTER else 1)
+    h = [1.0 / n0] * 3
+    L = [h[d] * (nglob[d] - (0 if center == CELL_CENTER else 1)) for d in range(3)]
+    rhs = _rhs(nglob)
+    ref = oracle_solve(nglob, 1, UNB3, h, L, center, kernel, rhs)
+    for precision, tol in ((64, 1e-12), (32, 2e-6)):
+        xl = gpu_solve(nglob, 1, UNB3, h, L, center, kernel, rhs, precision=precision, device=True)
+        xf = gpu_solve(nglob, 1, UNB3, h, L, center, kernel, rhs, precision=precision, device=True, xlast=False)
+        assert rel_l2(xl, ref) <= tol
+        assert rel_l2(xf, ref) <= tol
+        assert rel_l2(xl, xf) <= tol
+
+
+@pytest.mark.parametrize("n,odiff,kernel", [(32, 1, LGF_2), (48, 2, HEJ_2), (64, 4, CHAT_2)])
+def test_rot_xlast_matches_oracle(n, odiff, kernel):
+    """ROT solves of device arrays in the x-last order (fused rows, three
+    component warps per row meeting at a named barrier for the curl): FP64
+    against the oracle (<= 1e-12), FP32 against the FP64 mode (<= 2e-6)."""
+    from gpu_helpers import gpu_solve
+    nglob = [n] * 3
+    bcv = [[[4] * 3, [4] * 3]] * 3
+    h = [1.0 / n] * 3
+    L = [1.0] * 3
+    rhs = _rhs(nglob, 3, seed=13)
+    ref = oracle_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff)
+    got = gpu_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff, device=True)
+    assert rel_l2(got, ref) <= 1e-12
+    got32 = gpu_solve(nglob, 3, bcv, h, L, CELL_CENTER, kernel, rhs, type_=1, odiff=odiff, precision=32, device=True)
+    assert rel_l2(got32, got) <= 2e-6

@@ -61,13 +61,26 @@ def _grid(nglob, center):
     return h, L
 
 
-def _solve(nglob, lda, bcv, center, kernel, precision, rhs, type_=0, odiff=0):
+def _solve(nglob, lda, bcv, center, kernel, precision, rhs, type_=0, odiff=0, device=False):
+    """device=False: host arrays (the reference's pass order, slab-streamed);
+    device=True: CUDA arrays (the x-last order of all-unbounded problems),
+    whose passes plan_json describes."""
     h, L = _grid(nglob, center)
     t, s = make_solver(nglob, lda, bcv, h, L, center, kernel, odiff=odiff, precision=precision)
     plan = s.plan_json(type_)
     u = to_user(rhs)
-    out = np.zeros_like(u)
-    s.solve(out, u, type_)
+    if device:
+        import torch
+        du = torch.from_numpy(u).cuda()
+        dout = torch.zeros_like(du)
+        s.solve(dout, du, type_)
+        torch.cuda.synchronize()
+        out = dout.cpu().numpy()
+    else:
+        s.set_xlast(False)
+        plan = s.plan_json(type_)
+        out = np.zeros_like(u)
+        s.solve(out, u, type_)
     assert s.last_error() == 0
     return from_user(out, lda, nglob), plan
 
@@ -88,28 +101,43 @@ def _check_fast(plan, M, axis):
     assert all(p["fast"] for p in sel), sel
 
 
+@pytest.mark.parametrize("device", [False, True], ids=["host", "device"])
 @pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
 @pytest.mark.parametrize("name,nglob,bcv,center,kernel,M,axis", CASES, ids=[c[0] for c in CASES])
-def test_kernel_instance_matches_oracle(name, nglob, bcv, center, kernel, M, axis, precision, tol):
+def test_kernel_instance_matches_oracle(name, nglob, bcv, center, kernel, M, axis, precision, tol, device):
+    """Host arrays run the reference's pass order (x rows r2c / c2r, the fused
+    pass along z); device arrays of all-unbounded grids run the x-last order
+    (z columns r2c / c2r of the user's doubles, the fused pass along x rows)."""
     rhs = _rhs(nglob)
-    got, plan = _solve(nglob, 1, bcv, center, kernel, precision, rhs)
+    got, plan = _solve(nglob, 1, bcv, center, kernel, precision, rhs, device=device)
     _check_fast(plan, M, axis)
+    if device and bcv is UNB3 and M <= 1024:
+        assert plan["xlast"] == 1
+        fused = [p for p in plan["passes"] if p["name"] == "fused"]
+        assert fused[0]["axis"] == 0 and fused[0]["fast"] == 5
     ref = _oracle(name, nglob, 1, bcv, center, kernel, rhs)
     assert rel_l2(got, ref) <= tol
 
 
 @pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
-def test_rot_768_point_lines_lgf4(precision, tol):
+@pytest.mark.parametrize("nglob,device", [([32, 32, 384], False), ([384, 32, 32], True), ([64, 64, 64], True)],
+                         ids=["z768_host", "x768_device", "64cube_device"])
+def test_rot_lines_lgf4(nglob, device, precision, tol):
     """The ROT solve of the 384^3 vortex-ring workload (LGF_4, spectral curl)
-    on 768-point z lines: 32 x 32 x 384 cells, three components."""
-    nglob = [32, 32, 384]
+    with 768-point lines along its fused direction: host arrays run the
+    reference's order (fused column pass along z, col_rot_kernel), device
+    arrays the x-last order where it applies (fused rows, row_rot_kernel:
+    lines that fit one warp, i.e. up to 1024 points for powers of two, and
+    768 (FP32) or 384 (FP64) points for 3 x 2^k)."""
     bcv = [[[4] * 3, [4] * 3]] * 3
     rhs = _rhs(nglob, lda=3, seed=23)
-    got, plan = _solve(nglob, 3, bcv, CELL_CENTER, LGF_4, precision, rhs, type_=1, odiff=1)
+    got, plan = _solve(nglob, 3, bcv, CELL_CENTER, LGF_4, precision, rhs, type_=1, odiff=1, device=device)
     # the last direction: forward DFT, curl and Green's multiply, inverse DFT in one register-DFT pass
     fused = [p for p in plan["passes"] if p["name"] == "fused"]
-    assert len(fused) == 1 and fused[0]["fast"] == 1 and fused[0]["st"][0]["M"] == 768, fused
-    ref = _oracle("rot768", nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
+    assert len(fused) == 1 and fused[0]["fast"] in (1, 5), fused
+    if device and (precision == 32 or nglob[0] <= 256):
+        assert plan["xlast"] == 1 and fused[0]["fast"] == 5 and fused[0]["axis"] == 0
+    ref = _oracle(f"rot_{nglob}", nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
     assert rel_l2(got, ref) <= tol
 
 
@@ -120,8 +148,10 @@ def test_full_256_cube_fp64_matches_oracle():
     n = 256
     nglob = [n] * 3
     rhs = _rhs(nglob, seed=29)
-    got, plan = _solve(nglob, 1, UNB3, CELL_CENTER, CHAT_2, 64, rhs)
-    for axis in range(3):
-        _check_fast(plan, 2 * n, axis)
     ref = _oracle("full256", nglob, 1, UNB3, CELL_CENTER, CHAT_2, rhs)
-    assert rel_l2(got, ref) <= 1e-12
+    for device in (False, True):
+        got, plan = _solve(nglob, 1, UNB3, CELL_CENTER, CHAT_2, 64, rhs, device=device)
+        for axis in range(3):
+            _check_fast(plan, 2 * n, axis)
+        assert plan["xlast"] == (1 if device else 0)
+        assert rel_l2(got, ref) <= 1e-12

@@ -2,7 +2,8 @@
 the last forward direction on the library's copy streams, overlapped with
 the transforms of the other slabs.  The slab passes do the same per-line
 arithmetic as whole-array passes, so a solve with host arrays must equal the
-solve of the same data in device arrays bit for bit: one call, async calls
+solve of the same data in device arrays in the same (reference) pass order
+bit for bit: one call, async calls
 back to back (each with its own input), a batch, an in-place call, a
 vector ROT solve, and grids that run the general line pass instead of the
 register DFTs."""
@@ -28,7 +29,10 @@ def _setup(nglob, lda, bcv, center, kernel, precision, odiff=0):
     fact = 0 if center == CELL_CENTER else 1
     h = [1.0 / (nglob[0] - fact)] * 3
     L = [h[d] * (nglob[d] - fact) for d in range(3)]
-    return make_solver(nglob, lda, bcv, h, L, center, kernel, odiff=odiff, precision=precision)
+    t, s = make_solver(nglob, lda, bcv, h, L, center, kernel, odiff=odiff, precision=precision)
+    # host arrays stream in the reference's pass order: device arrays in the same order
+    s.set_xlast(False)
+    return t, s
 
 
 def _device_solve(s, u, type_=0, nbatch=1):
