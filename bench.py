@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
-    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "serve", "node513", "rot384", "slab"],
+    ap.add_argument("--workload", default="solve", choices=["solve", "batch", "group", "serve", "node513", "rot384", "slab"],
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
@@ -59,6 +59,8 @@ def parse():
                     help="slab: y passes that store into / load from every rank's column array over CUDA IPC "
                          "(peer; NCCL all-to-all if any rank cannot open the others' arrays), or NCCL all-to-all")
     ap.add_argument("--overlap", type=int, default=0, help="1: overlap the per-x-slab middle passes on three streams")
+    ap.add_argument("--rot", action="store_true",
+                    help="with --profile --grid: a ROT solve (three components, LGF_4, spectral curl)")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="with --profile: an all-unbounded grid NX x NY x NZ instead of n^3 (for ncu captures of one pass "
                          "length on a smaller array, e.g. 256 256 512 runs the 1024-point fused z pass on 1/4 of the lines)")
@@ -145,14 +147,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# DRAM bytes (read + write) per launch / algorithmic bytes per launch of each pass,
-# from one ncu capture of the same kernel on a smaller array: the fused z pass
-# (1024-point lines) on the 256 x 256 x 512 grid (1219.8 MB of DRAM traffic for
-# 1213.5 MB algorithmic), the other passes on 256^3; the traffic of a 512^3
-# launch is this ratio times its algorithmic bytes (traffic grows with the
-# lines processed)
-TRAFFIC_RATIO_256 = {"fused": 1219.8 / 1213.5, "fwd1": 369.0 / 404.2, "bwd1": 397.7 / 404.2,
-                     "fwd0": 228.8 / 269.1, "bwd0": 228.4 / 269.1}
+# DRAM bytes (read + write) per launch / algorithmic bytes per launch of each pass
+# of the 512^3 solve (x-last order), from ncu captures of the same kernel
+# instances on quarter-size grids: the fused x rows and the z r2c / c2r pair
+# passes on 512 x 128 x 512, the y passes on 128 x 512 x 512 (profiles/); the
+# traffic of a 512^3 launch is this ratio times its algorithmic bytes (traffic
+# grows with the lines processed).  Ratios below 1: the last writes of a launch
+# are still in L2 when it ends.
+TRAFFIC_RATIO_512 = {"fused": 1166281472 / 1211634404, "fwd1": 753636352 / 806879232, "bwd1": 781875968 / 806879232,
+                     "fwd0": 488390656 / 537395200, "bwd0": 488814336 / 537395200}
 
 
 def measured_peaks():
@@ -329,6 +332,67 @@ def run_batch(args):
                      "peak": peak, "unit": "GB/s", "frac": tot_bytes / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
                      "bytes_per_step": tot_bytes, "traffic": None},
         "setup_s": setup_s,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_group(args):
+    """Unevenly sized grids solved as one CUDA graph (flups_b200_solve_group):
+    one right-hand side on each of 14 all-unbounded cell-centred grids, two of
+    each size in {32, 48, 64, 96, 128, 192, 256}^3 (one HEJ_2, one LGF_2),
+    FP32, against the same 14 solves issued one after another on one stream.
+    One step = the 14 solves."""
+    import torch
+    from flups_b200 import pyflups as pf
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    sizes = [32, 48, 64, 96, 128, 192, 256]
+    keep, solvers, rhss, outs = [], [], [], []
+    for n in sizes:
+        for kernel in ("HEJ_2", "LGF_2"):
+            t, s, _ = make_solver(pf, n, kernel, 32, stream)
+            s.set_async(True)
+            keep.append(t)
+            solvers.append(s)
+            rhss.append(rhs_gaussians(n, seed=n, device=dev))
+            outs.append(torch.empty_like(rhss[-1]))
+    pts = sum(n ** 3 for n in sizes) * 2
+
+    def timed(fn, steps):
+        with torch.cuda.stream(stream):
+            for _ in range(max(3, args.warmup)):
+                fn()
+        stream.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in evs:
+            a.record(stream)
+            fn()
+            b.record(stream)
+        stream.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return float(np.mean(ms)), float(np.percentile(ms, 50)), float(np.percentile(ms, 99))
+
+    def sequential():
+        for s, o, r in zip(solvers, outs, rhss):
+            s.solve(o, r)
+
+    seq = timed(sequential, args.steps)
+    ref = [o.clone() for o in outs]
+    codes = []
+    grp = timed(lambda: codes.append(pf.solve_group(solvers, outs, rhss, stream=stream)), args.steps)
+    stream.synchronize()
+    same = all(torch.equal(a, b) for a, b in zip(outs, ref))
+    ms = grp[0]
+    line = {
+        "metric": METRIC, "value": pts / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Gaussian sums)",
+        "config": {"workload": "14 uneven all-unbounded cell-centred grids {32..256}^3 x {HEJ_2, LGF_2}, FP32, "
+                               "one CUDA graph (flups_b200_solve_group)", "grids": sizes},
+        "p50_ms": grp[1], "p99_ms": grp[2],
+        "compare_ms_per_step": {"sequential_14_solves_one_stream": seq[0], "group_graph": grp[0]},
+        "group_equals_sequential_bitwise": same, "codes_ok": all(c == 0 for c in codes),
     }
     print(json.dumps(line), flush=True)
 
@@ -642,28 +706,31 @@ def run_slab(args):
 
 def run_profile_grid(args):
     """FP32 solves of a seeded random right-hand side on an anisotropic all-unbounded
-    grid (cell-centred, h = 1/NX), for ncu captures; prints the mean solve time."""
+    grid (cell-centred, h = 1/NX), for ncu captures; prints the mean solve time.
+    --rot: a three-component ROT solve (LGF_4, spectral curl)."""
     import torch
     from flups_b200 import pyflups as pf
     nx, ny, nz = args.grid
     torch.cuda.set_device(0)
     B = pf.BoundaryType
-    t = pf.Topology(0, 1, [nx, ny, nz])
-    s = pf.Solver(t, [[B.UNB, B.UNB]] * 3, [1.0 / nx] * 3, [1.0, ny / nx, nz / nx])
-    s.set_green_type(pf.GreenType[args.kernel])
+    lda, typ = (3, 1) if args.rot else (1, 0)
+    t = pf.Topology(0, lda, [nx, ny, nz])
+    bc = [[[B.UNB] * lda, [B.UNB] * lda]] * 3 if args.rot else [[B.UNB, B.UNB]] * 3
+    s = pf.Solver(t, bc, [1.0 / nx] * 3, [1.0, ny / nx, nz / nx], order_diff=pf.DiffType.SPE if args.rot else pf.DiffType.NOD)
+    s.set_green_type(pf.GreenType["LGF_4" if args.rot else args.kernel])
     s.set_precision(32)
     s.setup()
     g = torch.Generator(device="cuda")
     g.manual_seed(7)
-    rhs = torch.randn((nz, ny, nx), dtype=torch.float64, device="cuda", generator=g)
+    rhs = torch.randn((lda, nz, ny, nx), dtype=torch.float64, device="cuda", generator=g)
     field = torch.empty_like(rhs)
     for _ in range(max(1, args.warmup)):
-        s.solve(field, rhs)
+        s.solve(field, rhs, typ)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        s.solve(field, rhs)
+        s.solve(field, rhs, typ)
     e1.record()
     torch.cuda.synchronize()
     print(json.dumps({"profile": True, "grid": [nx, ny, nz], "ms_per_step": e0.elapsed_time(e1) / args.steps}), flush=True)
@@ -673,6 +740,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "group":
+        run_group(args)
         return
     if args.workload == "batch":
         run_batch(args)
@@ -854,10 +924,10 @@ def main():
         "setup_s": {"fp32": setup32, "fp64": setup64},
         "roofline": {"bound": "hbm", "kernel": dom["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (TRAFFIC_RATIO_256[dom["name"]] * dom["bytes"]
-                                 if (n == 512 and args.kernel == "LGF_2" and dom["name"] in TRAFFIC_RATIO_256) else None),
-                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum of the same kernel on a smaller grid "
-                                       "(fused: 256x256x512, others: 256^3), scaled by lines",
+                     "traffic": (TRAFFIC_RATIO_512[dom["name"]] * dom["bytes"]
+                                 if (n == 512 and args.kernel == "LGF_2" and dom["name"] in TRAFFIC_RATIO_512) else None),
+                     "traffic_source": "ncu dram__bytes_read.sum+dram__bytes_write.sum of the same kernel instance on a "
+                                       "quarter-size grid (fused rows: 512x128x512), scaled by rows",
                      "bytes_per_launch": dom["bytes"], "ms_per_launch": dom_ms,
                      "solve_bytes": tot_bytes, "solve_frac": tot_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
                      "passes": [{"name": p["name"], "ms": p["ms_total"] / max(1, p["calls"]), "bytes": p["bytes"]} for p in stats]},

@@ -227,12 +227,31 @@ void flups_set_precision(Solver* s, int bits) {
 }
 int flups_get_precision(Solver* s) { return s->precision; }
 void flups_set_async(Solver* s, int async) { s->async = async != 0; }
-void flups_b200_set_fast_kernels(Solver* s, int on) { s->use_fast = on != 0; }
-void flups_b200_set_autotune(Solver* s, int on) { s->autotune = on != 0; }
-void flups_b200_set_overlap(Solver* s, int on) { s->overlap = on != 0; }
-void flups_b200_set_prefetch(Solver* s, int on) { s->prefetch = on != 0; }
-void flups_b200_set_xlast(Solver* s, int on) { s->xlast_on = on != 0; }
-void flups_b200_set_col_tile(Solver* s, int tile) { s->force_tile = (tile == 1 || tile == 2) ? tile : 0; }
+// switches that change the passes drop the captured solves
+void flups_b200_set_fast_kernels(Solver* s, int on) {
+    s->use_fast = on != 0;
+    s->drop_graphs();
+}
+void flups_b200_set_autotune(Solver* s, int on) {
+    s->autotune = on != 0;
+    s->drop_graphs();
+}
+void flups_b200_set_overlap(Solver* s, int on) {
+    s->overlap = on != 0;
+    s->drop_graphs();
+}
+void flups_b200_set_prefetch(Solver* s, int on) {
+    s->prefetch = on != 0;
+    s->drop_graphs();
+}
+void flups_b200_set_xlast(Solver* s, int on) {
+    s->xlast_on = on != 0;
+    s->drop_graphs();
+}
+void flups_b200_set_col_tile(Solver* s, int tile) {
+    s->force_tile = (tile == 1 || tile == 2) ? tile : 0;
+    s->drop_graphs();
+}
 int flups_solve_graph(Solver* s, double* field, double* rhs, int nbatch, int type) {
     if (!s) return -1;
     return s->solve_graph(field, rhs, type, nbatch);

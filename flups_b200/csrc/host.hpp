@@ -73,6 +73,12 @@ void sort_plans(DirPlan p[3]);
 
 }  // namespace flb
 
+struct Solver;
+namespace flb {
+// drops the group graphs (flups_b200_solve_group) that hold a solver being destroyed
+void group_forget(const Solver* s);
+}  // namespace flb
+
 // Opaque handles of the C API
 struct Topology {
     int axis = 0, lda = 1, nf = 1, alignment = FLUPS_ALIGNMENT;
@@ -173,6 +179,7 @@ struct Solver {
     std::map<GraphKey, cudaGraphExec_t> graphs;
     cudaStream_t capture_stream = nullptr;
     bool capturing = false;
+    uint64_t gen = 0;                     // bumped whenever captured solves become stale
     void drop_graphs();
     std::string pass_key(const flb::PassArgs& A, bool f64) const;
     void autotune_passes(int type, int nbatch);

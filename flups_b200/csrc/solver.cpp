@@ -239,6 +239,7 @@ void Solver::dry_run(DirPlan p[3]) {
 }
 
 Solver::~Solver() {
+    group_forget(this);
     drop_graphs();
     if (ov_stream[0]) {
         for (int i = 0; i < 2; ++i) {
@@ -1318,9 +1319,13 @@ void Solver::ensure_buffers(int nbatch) {
     buf_batch = std::max(buf_batch, nbatch);
 }
 
+// Captured solves (flups_solve_graph, and the group graphs that count on
+// `gen`) point at the work arrays and follow the switches in force when they
+// were captured: reallocation and switch changes drop them.
 void Solver::drop_graphs() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
+    ++gen;
 }
 
 size_t Solver::device_bytes(int nbatch) const {

@@ -135,6 +135,7 @@ def load_library(path=None):
         "flups_do_FFT": (None, [vp, vp, c_int]),
         "flups_do_mult": (None, [vp, vp, c_int]),
         "flups_solve_graph": (c_int, [vp, vp, vp, c_int, c_int]),
+        "flups_b200_solve_group": (c_int, [POINTER(vp), c_int, POINTER(vp), POINTER(vp), ip, vp]),
         "flups_get_last_error": (c_int, [vp]),
         "flups_get_device_bytes": (c_size_t, [vp, c_int]),
         "flups_b200_plan_json": (c_int, [vp, c_int, c_int, ctypes.c_char_p, c_int]),
@@ -436,3 +437,17 @@ def pencil_dirs(boundary_conditions):
     dirs = (c_int * 3)()
     lib.flups_pencilDirs(bc, dirs)
     return list(dirs)
+
+
+def solve_group(solvers, fields, rhss, types=None, stream=None):
+    """flups_b200_solve_group: the solves of several solvers (device arrays,
+    different grids allowed) as one CUDA graph on `stream` (a torch stream or
+    None); returns the library's code (0 on success)."""
+    n = len(solvers)
+    types = [int(SolverType.STD)] * n if types is None else [int(t) for t in types]
+    sv = (c_void_p * n)(*[s._solver for s in solvers])
+    fv = (c_void_p * n)(*[_ptr(f).value for f in fields])
+    rv = (c_void_p * n)(*[_ptr(r).value for r in rhss])
+    tv = (c_int * n)(*types)
+    st = c_void_p(stream.cuda_stream) if stream is not None else None
+    return _lib.flups_b200_solve_group(sv, n, fv, rv, tv, st)

@@ -176,6 +176,24 @@ int flups_b200_ipc_close(void* dev_ptr);
  * FFTW plans, src/Solver.cpp:1207-1272). */
 int flups_solve_graph(struct Solver* s, double* field, double* rhs, int nbatch, int type);
 
+/* Solves of n different solvers -- unevenly sized grids, other boundary
+ * conditions, kernels, precisions or solver types (STD / ROT) -- as ONE CUDA
+ * graph launched on `stream` (a cudaStream_t; NULL = the default stream).
+ * fields[i] and rhss[i] are device arrays of solver ss[i] (set up, not a
+ * z-slab share); a solver appears once (its work arrays are one set).  The
+ * first call for a given (solvers, arrays, types) runs each solve once,
+ * then captures them as independent branches of one graph, so the small
+ * grids' passes run side by side; later calls launch that graph (a member
+ * whose work arrays grew or whose switches changed gets the group
+ * recaptured; destroying a member drops its groups).  The call returns once
+ * the graph is queued: synchronise `stream` before reading the fields.
+ * Returns 0, -1 (bad arguments or a solver not set up), -2 (host pointers,
+ * a solver or an output twice) or -4 (CUDA error, in flups_get_last_error
+ * of every member).  No reference counterpart (the reference solves one
+ * field per call). */
+int flups_b200_solve_group(struct Solver* const* ss, int n, double* const* fields, double* const* rhss, const int* types,
+                           void* stream);
+
 /* One solve that allocates no device memory, for callers that cannot call
  * cudaMalloc while they run: real-time loops that must stay out of the
  * allocator (cudaMalloc can synchronise the device and takes driver locks,
