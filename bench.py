@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--overlap", type=int, default=0, help="1: overlap the per-x-slab middle passes on three streams")
     ap.add_argument("--rot", action="store_true",
                     help="with --profile --grid: a ROT solve (three components, LGF_4, spectral curl)")
+    ap.add_argument("--bcs", type=int, nargs=6, default=None, metavar="BC",
+                    help="with --profile --grid: boundary conditions x- x+ y- y+ z- z+ (0 EVEN, 1 ODD, 3 PER, 4 UNB)")
+    ap.add_argument("--node", action="store_true", help="with --profile --grid: node-centred data")
+    ap.add_argument("--precision", type=int, default=32, choices=[32, 64], help="with --profile --grid: working precision")
+    ap.add_argument("--no-xlast", action="store_true", help="with --profile --grid: the reference's pass order")
     ap.add_argument("--grid", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="with --profile: an all-unbounded grid NX x NY x NZ instead of n^3 (for ncu captures of one pass "
                          "length on a smaller array, e.g. 256 256 512 runs the 1024-point fused z pass on 1/4 of the lines)")
@@ -715,10 +720,17 @@ def run_profile_grid(args):
     B = pf.BoundaryType
     lda, typ = (3, 1) if args.rot else (1, 0)
     t = pf.Topology(0, lda, [nx, ny, nz])
-    bc = [[[B.UNB] * lda, [B.UNB] * lda]] * 3 if args.rot else [[B.UNB, B.UNB]] * 3
-    s = pf.Solver(t, bc, [1.0 / nx] * 3, [1.0, ny / nx, nz / nx], order_diff=pf.DiffType.SPE if args.rot else pf.DiffType.NOD)
+    b6 = args.bcs if args.bcs else [4] * 6
+    bc = [[[b6[2 * d]] * lda, [b6[2 * d + 1]] * lda] for d in range(3)]
+    m = nx - 1 if args.node else nx
+    L = [1.0, (ny - (1 if args.node else 0)) / m, (nz - (1 if args.node else 0)) / m]
+    ctr = pf.CenterType.NODE_CENTER if args.node else pf.CenterType.CELL_CENTER
+    s = pf.Solver(t, bc, [1.0 / m] * 3, L, order_diff=pf.DiffType.SPE if args.rot else pf.DiffType.NOD,
+                  center_type=[ctr] * 3)
     s.set_green_type(pf.GreenType["LGF_4" if args.rot else args.kernel])
-    s.set_precision(32)
+    s.set_precision(args.precision)
+    if args.no_xlast:
+        s.set_xlast(False)
     s.setup()
     g = torch.Generator(device="cuda")
     g.manual_seed(7)

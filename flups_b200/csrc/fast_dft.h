@@ -138,6 +138,15 @@ __host__ __device__ constexpr int fast_radix1_row(int n, int f64) {
 __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
     return (mode < 2 && fast_radix48(n, f64)) ? 48 : ((n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
 }
+// the fused ROT rows (row_rot_kernel): FP32 384- and 768-point lines with a first
+// radix of 48 (two Stockham stages, one exchange per DFT instead of two; 168
+// registers, 28 bytes spilled), else the fused passes' radix
+#ifndef FLB_ROWROT_R48
+#define FLB_ROWROT_R48 1
+#endif
+__host__ __device__ constexpr int fast_radix1_rowrot(int n, int f64) {
+    return (FLB_ROWROT_R48 && fast_radix48(n, f64)) ? 48 : fast_radix1_mode(n, f64, 2);
+}
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix
 __host__ __device__ constexpr int fast_gcd(int a, int b) { return b == 0 ? a : fast_gcd(b, a % b); }

@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
 
 template <typename T, int L, int NT, int SH>
 inline cudaError_t launch_row_rot_t(const RowFusedArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, 2);
+    constexpr int R1 = fast_radix1_rowrot(L, sizeof(T) == 8);
     using F = RegFFT<T, L, R1, true, true, true>;
     constexpr int LPW = 32 / F::P;
     constexpr size_t smem = (size_t)NT * LPW * (3 * F::SC * sizeof(typename CT<T>::C) + RowFusedTile<T, L>::GP * sizeof(T));

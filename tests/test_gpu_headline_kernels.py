@@ -120,8 +120,9 @@ def test_kernel_instance_matches_oracle(name, nglob, bcv, center, kernel, M, axi
 
 
 @pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
-@pytest.mark.parametrize("nglob,device", [([32, 32, 384], False), ([384, 32, 32], True), ([64, 64, 64], True)],
-                         ids=["z768_host", "x768_device", "64cube_device"])
+@pytest.mark.parametrize("nglob,device", [([32, 32, 384], False), ([384, 32, 32], True), ([192, 32, 32], True),
+                                          ([64, 64, 64], True)],
+                         ids=["z768_host", "x768_device", "x384_device", "64cube_device"])
 def test_rot_lines_lgf4(nglob, device, precision, tol):
     """The ROT solve of the 384^3 vortex-ring workload (LGF_4, spectral curl)
     with 768-point lines along its fused direction: host arrays run the
