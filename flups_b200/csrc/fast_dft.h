@@ -147,6 +147,14 @@ __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
 __host__ __device__ constexpr int fast_radix1_rowrot(int n, int f64) {
     return (FLB_ROWROT_R48 && fast_radix48(n, f64)) ? 48 : fast_radix1_mode(n, f64, 2);
 }
+// the half-length DCT / DST rows (row_dct_kernel): the LH-point DFT's first
+// radix (FLB_DCT_R1 > 0 overrides it for FP32 power-of-two lines it divides)
+#ifndef FLB_DCT_R1
+#define FLB_DCT_R1 0
+#endif
+__host__ __device__ constexpr int fast_radix1_dct(int lh, int f64) {
+    return (FLB_DCT_R1 > 0 && !f64 && lh % 3 != 0 && lh % FLB_DCT_R1 == 0 && lh / FLB_DCT_R1 <= 32) ? FLB_DCT_R1 : fast_radix1_of(lh, f64);
+}
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix
 __host__ __device__ constexpr int fast_gcd(int a, int b) { return b == 0 ? a : fast_gcd(b, a % b); }

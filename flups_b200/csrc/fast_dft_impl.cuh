@@ -1339,8 +1339,17 @@ struct DctW4 {
     static constexpr int N = SM ? USED : 0;
 };
 
+// CTAs per SM the DCT rows ask the compiler for (FLB_DCT_MINB > 0 overrides)
+#ifndef FLB_DCT_MINB
+#define FLB_DCT_MINB 0
+#endif
+template <int THREADS>
+struct DctOcc {
+    static constexpr int blocks = FLB_DCT_MINB > 0 ? FLB_DCT_MINB : Occ<THREADS>::blocks;
+};
+
 template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
-__global__ void __launch_bounds__(TR * (LH / R1), (Occ<TR * (LH / R1)>::blocks)) row_dct_kernel(const RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), DctOcc<TR * (LH / R1)>::blocks) row_dct_kernel(const RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     constexpr int P = F::P, N = 2 * LH;
@@ -1794,7 +1803,7 @@ inline cudaError_t launch_r2r_len(int M, const RowArgs& a, int ncomp, cudaStream
 
 template <typename T, typename IT, typename OT, int LH, int FAM>
 inline cudaError_t launch_dct_t(const RowArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = fast_radix1_of(LH, sizeof(T) == 8);
+    constexpr int R1 = fast_radix1_dct(LH, sizeof(T) == 8);
     using F = RegFFT<T, LH, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem =

@@ -166,7 +166,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             slot_for(2 * A.st[0].M, 0);
             if (fast_dct_family(sp.kind, sp.n_in, A.st[0].M)) {
                 slot_for(sp.n_in, 0);
-                slot_for(sp.n_in / 2, r1_of(sp.n_in / 2));
+                slot_for(sp.n_in / 2, fast_radix1_dct(sp.n_in / 2, f64 ? 1 : 0));
             } else {
                 slot_for(A.st[0].M, r1_of(A.st[0].M));
             }
@@ -224,7 +224,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                     r.tw2 = tw_of(2 * L, 0);
                     if (fast_dct_family(r.kind, r.n, L)) {
                         r.tw = tw_of(r.n, 0);
-                        r.tws = tw_of(r.n / 2, r1_of(r.n / 2));
+                        r.tws = tw_of(r.n / 2, fast_radix1_dct(r.n / 2, f64 ? 1 : 0));
                     } else {
                         r.tws = tw_of(L, r1_of(L));
                     }

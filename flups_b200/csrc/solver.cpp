@@ -765,7 +765,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         r.tw2 = twiddle(L, f64);
         if (fast_dct_family(r.kind, r.n, L)) {
             r.tw = twiddle_plain(r.n, f64);
-            r.tws = stage_table(r.n / 2, f64);
+            r.tws = stage_table(r.n / 2, f64, fast_radix1_dct(r.n / 2, f64 ? 1 : 0));
         } else {
             r.tws = stage_table(L, f64);
         }
