@@ -14,12 +14,14 @@ Reported (one JSON line on rank 0):
              (H2D of the RHS and D2H of the field inside every step)
   roofline   the dominant pass: algorithmic bytes per launch / its average
              CUDA-event duration, against the measured HBM copy bandwidth
-  cpu_baseline  the CPU oracle (numpy/scipy restatement of the reference
-             solver) on a bounded 128^3 sample, all host threads
+  cpu_baseline  the reference's own solver (its sources compiled unmodified
+             by oracle/build_ref.py against in-repo FFTW/MPI/h3lpr stand-ins,
+             one rank, OpenMP on all host threads) on a bounded 128^3 sample;
+             the oracle port (numpy/scipy) when that build is absent
 
---impl reference times the reference's CPU algorithm (the oracle port: the
-reference needs FFTW, MPI and h3lpr, which this image does not have) on the
-same metric.  --gpus N runs N independent replicas (one per GPU, weak
+--impl reference times the same reference build on the same metric, at the
+workload's full grid when its run fits in about four minutes and half the
+free host memory, else on a 256^3 or 128^3 sample.  --gpus N runs N independent replicas (one per GPU, weak
 scaling).  --workload slab instead splits one solve over the ranks by z
 planes (flups_b200/slab.py: NCCL all-to-all of the spectrum; strong scaling).
 """
@@ -171,53 +173,96 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_oracle_sample(n, kernel, steps=3):
-    """Time the CPU oracle (FP64, all host threads) on an n^3 sample; returns pts/s and details."""
-    import scipy.fft as sfft
+REF_KIND_DESC = {
+    "reference": "the reference's own solver (its src/*.cpp compiled unmodified, one rank, OpenMP on all host "
+                 "threads) on an in-repo FP64 FFT in place of FFTW (absent here), oracle/_ref/libflups_ref.so",
+    "port": "the reference's algorithm restated in numpy/scipy (FP64, all host threads); the reference build "
+            "oracle/_ref/libflups_ref.so was absent",
+}
 
+
+def _cpu_solver(n, kernel):
+    """A CPU solver of the n^3 all-unbounded cell-centred workload: the reference
+    build when it is present (kind "reference"), else the oracle port."""
+    from oracle import ref_lib
     from oracle.plans import CELL_CENTER
-    from oracle.solver import OracleSolver
     from flups_b200.pyflups import GreenType
-    ncores = os.cpu_count() or 1
-    o = OracleSolver([n] * 3, 1, [[[4], [4]]] * 3, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER)
+    bc = [[[4], [4]]] * 3
+    if ref_lib.available():
+        return ref_lib.RefSolver([n] * 3, 1, bc, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER, int(GreenType[kernel])), "reference"
+    from oracle.solver import OracleSolver
+    o = OracleSolver([n] * 3, 1, bc, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER)
     o.green_type = int(GreenType[kernel])
     o.setup()
+    return o, "port"
+
+
+def _cpu_time(solver, rhs):
+    import scipy.fft as sfft
+    with sfft.set_workers(os.cpu_count() or 1):
+        t0 = time.perf_counter()
+        solver.solve(rhs)
+        return time.perf_counter() - t0
+
+
+def cpu_oracle_sample(n, kernel, steps=3):
+    """Time the CPU baseline (the reference build, else the oracle port) on an
+    n^3 sample of the workload; returns pts/s, cores, median seconds, kind."""
+    cores = os.cpu_count() or 1
+    solver, kind = _cpu_solver(n, kernel)
     rhs = rhs_gaussians(n)[None].transpose(0, 3, 2, 1).copy()
-    times = []
-    with sfft.set_workers(ncores):
-        o.solve(rhs)
-        for _ in range(steps):
-            t0 = time.perf_counter()
-            o.solve(rhs)
-            times.append(time.perf_counter() - t0)
+    _cpu_time(solver, rhs)
+    times = [_cpu_time(solver, rhs) for _ in range(steps)]
     t = float(np.median(times))
-    return n ** 3 / t, ncores, t
+    return n ** 3 / t, cores, t, kind
+
+
+def _mem_available():
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def reference_sample_n(args):
+    """The largest of n, 256, 128 (n = the workload's grid) whose reference run
+    (set-up + warm-up + timed solves) is predicted to end within about four
+    minutes and whose arrays fit in half the free host memory, from one timed
+    64^3 set-up and solve (time and memory grow with the point count, times a
+    log factor)."""
+    solver, _ = _cpu_solver(64, args.kernel)
+    rhs = rhs_gaussians(64)[None].transpose(0, 3, 2, 1).copy()
+    _cpu_time(solver, rhs)
+    t64 = _cpu_time(solver, rhs)
+    del solver
+    mem = _mem_available()
+    for n in (args.n, 256, 128):
+        if n > args.n:
+            continue
+        f = (n / 64) ** 3 * (1.0 + np.log2(n / 64) / 6.0)
+        t_total = (3.0 + args.warmup + args.steps) * t64 * f  # set-up counted as three solves
+        need = 300.0 * (n ** 3) + 16.0 * n ** 3  # measured ~270 B per point in the reference build, + dense copies
+        if t_total < 240.0 and (mem == 0 or need < 0.5 * mem):
+            return n
+    return 128
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n = args.sample_n
-    pts, cores, t = None, None, None
-    times = []
-    import scipy.fft as sfft
-
-    from oracle.plans import CELL_CENTER
-    from oracle.solver import OracleSolver
-    from flups_b200.pyflups import GreenType
+    n = reference_sample_n(args)
     cores = os.cpu_count() or 1
-    o = OracleSolver([n] * 3, 1, [[[4], [4]]] * 3, [1.0 / n] * 3, [1.0] * 3, CELL_CENTER)
-    o.green_type = int(GreenType[args.kernel])
-    o.setup()
+    t0 = time.perf_counter()
+    solver, kind = _cpu_solver(n, args.kernel)
+    setup_s = time.perf_counter() - t0
     rhs = rhs_gaussians(n)[None].transpose(0, 3, 2, 1).copy()
-    with sfft.set_workers(cores):
-        for _ in range(args.warmup):
-            o.solve(rhs)
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            o.solve(rhs)
-            times.append(time.perf_counter() - t0)
+    for _ in range(args.warmup):
+        _cpu_time(solver, rhs)
+    times = [_cpu_time(solver, rhs) for _ in range(args.steps)]
     tot = sum(times)
     value = args.steps * n ** 3 / tot
     line = {
@@ -226,10 +271,11 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian sum)",
         "config": {"workload": f"{args.n}^3 cell-centred all-unbounded Poisson, {args.kernel}", "sample": f"{n}^3",
                    "l2_flush": "host run"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n}^3 solves of the same workload (the reference's algorithm restated in numpy/scipy, FP64; FFTW/MPI absent here)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{n}^3 solves of the same workload: {REF_KIND_DESC[kind]}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "p50_ms": float(np.percentile(times, 50) * 1e3), "p99_ms": float(np.percentile(times, 99) * 1e3),
+        "setup_s": setup_s,
     }
     print(json.dumps(line), flush=True)
 
@@ -918,7 +964,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    cpu_value, cores, cpu_t = cpu_oracle_sample(args.sample_n, args.kernel)
+    cpu_value, cores, cpu_t, cpu_kind = cpu_oracle_sample(args.sample_n, args.kernel)
     ms_per_step = elapsed / args.steps
     value = world * n ** 3 / (ms_per_step * 1e-3)
     clocks = clk.summary()
@@ -949,8 +995,8 @@ def main():
                 "pcie_bound_ms": pcie_ms,
                 "pcie_bound_note": "the step's H2D and D2H bytes copied at once on two streams, no solve"},
         "gpu_launches": launches_per_solve * args.steps,
-        "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.sample_n}^3 solves of the same workload, FP64 oracle (numpy/scipy restatement), median of 3"},
+        "cpu_baseline": {"value": cpu_value, "unit": UNIT, "cores": cores, "kind": cpu_kind,
+                         "sample": f"{args.sample_n}^3 solves of the same workload, median of 3: {REF_KIND_DESC[cpu_kind]}"},
         "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
