@@ -148,12 +148,23 @@ __host__ __device__ constexpr int fast_radix1_rowrot(int n, int f64) {
     return (FLB_ROWROT_R48 && fast_radix48(n, f64)) ? 48 : fast_radix1_mode(n, f64, 2);
 }
 // the half-length DCT / DST rows (row_dct_kernel): the LH-point DFT's first
-// radix (FLB_DCT_R1 > 0 overrides it for FP32 power-of-two lines it divides)
+// radix.  FP32 power-of-two lines up to 256 points take 16 (16 complex values
+// per lane, 64 registers, four 256-thread CTAs per SM: 513 x 257 x 257 node
+// grid, DCT-III rows 0.167 -> 0.134 ms, DCT-II rows 0.134 -> 0.115 ms against
+// a first radix of 32 at two CTAs per SM); FLB_DCT_R1 / FLB_DCT_R1_F64 set
+// the FP32 / FP64 radix of the power-of-two lines it divides (0: the column
+// passes' radix).
 #ifndef FLB_DCT_R1
-#define FLB_DCT_R1 0
+#define FLB_DCT_R1 16
+#endif
+#ifndef FLB_DCT_R1_F64
+#define FLB_DCT_R1_F64 0
 #endif
 __host__ __device__ constexpr int fast_radix1_dct(int lh, int f64) {
-    return (FLB_DCT_R1 > 0 && !f64 && lh % 3 != 0 && lh % FLB_DCT_R1 == 0 && lh / FLB_DCT_R1 <= 32) ? FLB_DCT_R1 : fast_radix1_of(lh, f64);
+    return ((f64 ? FLB_DCT_R1_F64 : FLB_DCT_R1) > 0 && lh % 3 != 0 && lh % (f64 ? FLB_DCT_R1_F64 : FLB_DCT_R1) == 0 &&
+            lh / (f64 ? FLB_DCT_R1_F64 : FLB_DCT_R1) <= 16)
+               ? (f64 ? FLB_DCT_R1_F64 : FLB_DCT_R1)
+               : fast_radix1_of(lh, f64);
 }
 // radix of a later Stockham stage: the largest common divisor of what is left
 // of the line (n / Ns) and the first radix

@@ -704,9 +704,21 @@ __global__ void __launch_bounds__(WARPS * 32, RowFusedOcc<T>::blocks) row_fused_
 #ifndef FLB_ROWROT_TRIPLES
 #define FLB_ROWROT_TRIPLES 2
 #endif
+#ifndef FLB_ROWROT_PAIRED
+#define FLB_ROWROT_PAIRED 0
+#endif
+// threads per SM the ROT rows ask the compiler for (FLB_ROWROT_PER_SM > 0
+// overrides the fused rows' figure)
+#ifndef FLB_ROWROT_PER_SM
+#define FLB_ROWROT_PER_SM 0
+#endif
+template <typename T, int NT>
+struct RowRotOcc {
+    static constexpr int per_sm = FLB_ROWROT_PER_SM > 0 ? FLB_ROWROT_PER_SM : RowFusedOcc<T>::per_sm;
+    static constexpr int blocks = per_sm / (NT * 96) > 0 ? per_sm / (NT * 96) : 1;
+};
 template <typename T, int L, int R1, int NT, int SH>
-__global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 0 ? RowFusedOcc<T>::per_sm / (NT * 96) : 1)
-    row_rot_kernel(const __grid_constant__ RowFusedArgs a) {
+__global__ void __launch_bounds__(NT * 96, RowRotOcc<T, NT>::blocks) row_rot_kernel(const __grid_constant__ RowFusedArgs a) {
     using F = RegFFT<T, L, R1, true, true, true>;
     using C = typename CT<T>::C;
     constexpr int P = F::P, LPW = 32 / P, GP = RowFusedTile<T, L>::GP;
@@ -773,13 +785,30 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
         if (at(ga) == a.nyq[ga]) sb = (T)1;
     }
     __syncwarp();
+    // the spectra meet in the lines in a layout of the curl's own: FP32 values
+    // r, r+1 of lane p side by side (one 16-byte access), else mode order
+    constexpr bool PAIRED = FLB_ROWROT_PAIRED && sizeof(T) == 4 && R1 % 2 == 0;
+    if constexpr (PAIRED) {
+        float4* l4 = reinterpret_cast<float4*>(line);
 #pragma unroll
-    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+        for (int r = 0; r < R1; r += 2) l4[(r / 2) * P + p] = make_float4(v[r].x, v[r].y, v[r + 1].x, v[r + 1].y);
+    } else {
+#pragma unroll
+        for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
+    }
     if (g == 0) cp_async_wait_all();
     asm volatile("bar.sync %0, 96;" ::"r"(1 + tri) : "memory");
     {
         const C* fa = line_of(ga);
         const C* fb = line_of(gb);
+        auto spec = [&](const C* f, int r) -> C {
+            if constexpr (PAIRED) {
+                const float4 q = reinterpret_cast<const float4*>(f)[(r / 2) * P + p];
+                return (r & 1) ? mkc((T)q.z, (T)q.w) : mkc((T)q.x, (T)q.y);
+            } else {
+                return f[F::sw(p + P * r)];
+            }
+        };
         auto curl = [&](auto mode) {
             constexpr int VARY = decltype(mode)::value;
 #pragma unroll
@@ -787,7 +816,7 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
                 const int k = p + P * r;
                 const C A = (VARY == 1) ? __ldg(ktab + k) : ka;
                 const C B = (VARY == 2) ? __ldg(ktab + k) : kb;
-                const C wa = fa[F::sw(k)], wb = fb[F::sw(k)];
+                const C wa = spec(fa, r), wb = spec(fb, r);
                 C u = csub(cmul(wa, A), cmul(wb, B));
                 // kx >= L/2 and kx = 0: the reference's form (see above); the
                 // line's own symbol flips sign at -k except at kx = L/2
@@ -1339,17 +1368,24 @@ struct DctW4 {
     static constexpr int N = SM ? USED : 0;
 };
 
-// CTAs per SM the DCT rows ask the compiler for (FLB_DCT_MINB > 0 overrides)
+// CTAs per SM the DCT rows ask the compiler for: four for FP32 lines of a
+// first radix up to 16 (64 registers), else the column passes' figure;
+// FLB_DCT_MINB / FLB_DCT_MINB_F64 > 0 override it for FP32 / FP64
 #ifndef FLB_DCT_MINB
 #define FLB_DCT_MINB 0
 #endif
-template <int THREADS>
+#ifndef FLB_DCT_MINB_F64
+#define FLB_DCT_MINB_F64 0
+#endif
+template <typename T, int R1, int THREADS>
 struct DctOcc {
-    static constexpr int blocks = FLB_DCT_MINB > 0 ? FLB_DCT_MINB : Occ<THREADS>::blocks;
+    static constexpr int over = sizeof(T) == 8 ? FLB_DCT_MINB_F64 : FLB_DCT_MINB;
+    static constexpr int dflt = (sizeof(T) == 4 && R1 <= 16 && THREADS == 256) ? 4 : Occ<THREADS>::blocks;
+    static constexpr int blocks = over > 0 ? over : dflt;
 };
 
 template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
-__global__ void __launch_bounds__(TR * (LH / R1), DctOcc<TR * (LH / R1)>::blocks) row_dct_kernel(const RowArgs a) {
+__global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>::blocks) row_dct_kernel(const RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
     using C = typename CT<T>::C;
     constexpr int P = F::P, N = 2 * LH;
