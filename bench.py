@@ -19,6 +19,10 @@ Reported (one JSON line on rank 0):
              one rank, OpenMP on all host threads) on a bounded 128^3 sample;
              the oracle port (numpy/scipy) when that build is absent
 
+  configs    (one GPU) the other measured configurations run after the
+             headline in the same process: node513, rot384 and the 64 x 128^3
+             batch, one compact record each (--no-configs leaves them out)
+
 --impl reference times the same reference build on the same metric, at the
 workload's full grid when its run fits in about four minutes and half the
 free host memory, else on a 256^3 or 128^3 sample.  --gpus N runs N independent replicas (one per GPU, weak
@@ -53,6 +57,9 @@ def parse():
     ap.add_argument("--kernel", default="LGF_2")
     ap.add_argument("--sample-n", type=int, default=128, help="grid of the bounded CPU sample")
     ap.add_argument("--profile", action="store_true", help="FP32 solves only (for ncu captures): no FP64, e2e or CPU legs")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="solve workload: leave out the other measured configurations (node513, rot384, batch) "
+                         "that the default single-GPU line carries under 'configs'")
     ap.add_argument("--workload", default="solve", choices=["solve", "batch", "group", "serve", "node513", "rot384", "slab"],
                     help="solve: the 512^3 headline; batch: 64 RHS of 128^3 HEJ_2 FP32 sharing one Green's spectrum; "
                          "serve: 2000 requests of mixed sizes/BCs/kernels/precisions at 500 req/s")
@@ -231,9 +238,13 @@ def reference_sample_n(args):
     """The largest of n, 256, 128 (n = the workload's grid) whose reference run
     (set-up + warm-up + timed solves) is predicted to end within about four
     minutes and whose arrays fit in half the free host memory, from one timed
-    64^3 set-up and solve (time and memory grow with the point count, times a
-    log factor)."""
+    64^3 set-up and solve.  Solves grow with the point count times a log
+    factor, the set-up (the lattice Green's function evaluated point by point)
+    with the point count: 4.4 / 9.6 / 32.8 s at 96^3 / 128^3 / 192^3 on 8
+    cores, 460 s at 512^3 on 16 cores, against 18 s per 512^3 solve."""
+    t0 = time.perf_counter()
     solver, _ = _cpu_solver(64, args.kernel)
+    ts64 = time.perf_counter() - t0
     rhs = rhs_gaussians(64)[None].transpose(0, 3, 2, 1).copy()
     _cpu_time(solver, rhs)
     t64 = _cpu_time(solver, rhs)
@@ -242,8 +253,8 @@ def reference_sample_n(args):
     for n in (args.n, 256, 128):
         if n > args.n:
             continue
-        f = (n / 64) ** 3 * (1.0 + np.log2(n / 64) / 6.0)
-        t_total = (3.0 + args.warmup + args.steps) * t64 * f  # set-up counted as three solves
+        pts = (n / 64) ** 3
+        t_total = (args.warmup + args.steps) * t64 * pts * (1.0 + np.log2(n / 64) / 4.0) + ts64 * pts
         need = 300.0 * (n ** 3) + 16.0 * n ** 3  # measured ~270 B per point in the reference build, + dense copies
         if t_total < 240.0 and (mem == 0 or need < 0.5 * mem):
             return n
@@ -308,7 +319,7 @@ def rhs_batch_gaussians(n, nb, seed=4, device=None):
     return out
 
 
-def run_batch(args):
+def run_batch(args, emit=True):
     """64 right-hand sides of 128^3 (cell, all unbounded, HEJ_2, FP32) sharing one
     Green's spectrum: 64 sequential solves, one batched launch per pass with the
     default and the autotuned CTA tiles, and the autotuned batch replayed from a
@@ -384,7 +395,9 @@ def run_batch(args):
                      "bytes_per_step": tot_bytes, "traffic": None},
         "setup_s": setup_s,
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_group(args):
@@ -499,7 +512,7 @@ def fast_flags(stats, plan):
     return [by_name.get(p["name"], 0) for p in stats]
 
 
-def run_config(args):
+def run_config(args, emit=True):
     """node513 (node-centred 513x257x257, EVEN/ODD x, PER y, UNB z, HEJ_4) or
     rot384 (384^3 cell, all UNB, LGF_4, ROT with the spectral curl, 3 components):
     FP32 and FP64 solves of device arrays, the FP32 error against the FP64 mode,
@@ -582,7 +595,9 @@ def run_config(args):
                      "unit": "GB/s", "frac": tot / (ms32 * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None},
         "detail": res,
     }
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def run_serve(args):
@@ -1002,9 +1017,46 @@ def main():
                          "sample": f"{args.sample_n}^3 solves of the same workload, median of 3: {REF_KIND_DESC[cpu_kind]}"},
         "clocks": clocks,
     }
+    if world == 1 and not args.no_configs and n == 512:
+        line["configs"] = other_configs(args)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def other_configs(args):
+    """The other measured configurations, run after the headline in the same
+    process and carried on its line (one compact record each): node513
+    (513x257x257 node-centred EVEN/ODD-PER-UNB HEJ_4), rot384 (384^3 LGF_4 ROT,
+    three components) and batch (64 x 128^3 HEJ_2 sharing one Green's
+    spectrum, autotuned tiles, replayed graph).  Each is timed with CUDA events
+    on its own stream over 10 steps after 3 warm-ups; a failure is recorded,
+    not raised."""
+    import copy
+
+    import torch
+    out = {}
+    for name in ("node513", "rot384", "batch"):
+        a = copy.copy(args)
+        a.workload, a.steps, a.warmup = name, 10, 3
+        torch.cuda.empty_cache()
+        try:
+            ln = run_batch(a, emit=False) if name == "batch" else run_config(a, emit=False)
+        except Exception as e:  # noqa: BLE001 - a record of the failure is the result
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+            continue
+        rec = {"workload": ln["config"]["workload"], "value": ln["value"], "unit": ln["unit"],
+               "ms_per_step": ln["ms_per_step"], "p50_ms": ln.get("p50_ms"), "p99_ms": ln.get("p99_ms"),
+               "accuracy": ln.get("accuracy"), "roofline_frac": ln["roofline"]["frac"],
+               "roofline_kernel": ln["roofline"]["kernel"], "peak_kind": ln["roofline"]["peak_kind"]}
+        if "fp64" in ln:
+            rec["fp64_ms_per_step"] = ln["fp64"]["ms_per_step"]
+        if "detail" in ln:
+            rec["passes_ms"] = {p["name"]: p["ms"] for p in ln["detail"][32]["passes"]}
+        if "compare_ms_per_batch" in ln:
+            rec["compare_ms_per_batch"] = ln["compare_ms_per_batch"]
+        out[name] = rec
+    return out
 
 
 if __name__ == "__main__":

@@ -704,21 +704,10 @@ __global__ void __launch_bounds__(WARPS * 32, RowFusedOcc<T>::blocks) row_fused_
 #ifndef FLB_ROWROT_TRIPLES
 #define FLB_ROWROT_TRIPLES 2
 #endif
-#ifndef FLB_ROWROT_PAIRED
-#define FLB_ROWROT_PAIRED 0
-#endif
-// threads per SM the ROT rows ask the compiler for (FLB_ROWROT_PER_SM > 0
-// overrides the fused rows' figure)
-#ifndef FLB_ROWROT_PER_SM
-#define FLB_ROWROT_PER_SM 0
-#endif
-template <typename T, int NT>
-struct RowRotOcc {
-    static constexpr int per_sm = FLB_ROWROT_PER_SM > 0 ? FLB_ROWROT_PER_SM : RowFusedOcc<T>::per_sm;
-    static constexpr int blocks = per_sm / (NT * 96) > 0 ? per_sm / (NT * 96) : 1;
-};
+
 template <typename T, int L, int R1, int NT, int SH>
-__global__ void __launch_bounds__(NT * 96, RowRotOcc<T, NT>::blocks) row_rot_kernel(const __grid_constant__ RowFusedArgs a) {
+__global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 0 ? RowFusedOcc<T>::per_sm / (NT * 96) : 1)
+    row_rot_kernel(const __grid_constant__ RowFusedArgs a) {
     using F = RegFFT<T, L, R1, true, true, true>;
     using C = typename CT<T>::C;
     constexpr int P = F::P, LPW = 32 / P, GP = RowFusedTile<T, L>::GP;
@@ -785,30 +774,13 @@ __global__ void __launch_bounds__(NT * 96, RowRotOcc<T, NT>::blocks) row_rot_ker
         if (at(ga) == a.nyq[ga]) sb = (T)1;
     }
     __syncwarp();
-    // the spectra meet in the lines in a layout of the curl's own: FP32 values
-    // r, r+1 of lane p side by side (one 16-byte access), else mode order
-    constexpr bool PAIRED = FLB_ROWROT_PAIRED && sizeof(T) == 4 && R1 % 2 == 0;
-    if constexpr (PAIRED) {
-        float4* l4 = reinterpret_cast<float4*>(line);
 #pragma unroll
-        for (int r = 0; r < R1; r += 2) l4[(r / 2) * P + p] = make_float4(v[r].x, v[r].y, v[r + 1].x, v[r + 1].y);
-    } else {
-#pragma unroll
-        for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
-    }
+    for (int r = 0; r < R1; ++r) line[F::sw(p + P * r)] = v[r];
     if (g == 0) cp_async_wait_all();
     asm volatile("bar.sync %0, 96;" ::"r"(1 + tri) : "memory");
     {
         const C* fa = line_of(ga);
         const C* fb = line_of(gb);
-        auto spec = [&](const C* f, int r) -> C {
-            if constexpr (PAIRED) {
-                const float4 q = reinterpret_cast<const float4*>(f)[(r / 2) * P + p];
-                return (r & 1) ? mkc((T)q.z, (T)q.w) : mkc((T)q.x, (T)q.y);
-            } else {
-                return f[F::sw(p + P * r)];
-            }
-        };
         auto curl = [&](auto mode) {
             constexpr int VARY = decltype(mode)::value;
 #pragma unroll
@@ -816,7 +788,7 @@ __global__ void __launch_bounds__(NT * 96, RowRotOcc<T, NT>::blocks) row_rot_ker
                 const int k = p + P * r;
                 const C A = (VARY == 1) ? __ldg(ktab + k) : ka;
                 const C B = (VARY == 2) ? __ldg(ktab + k) : kb;
-                const C wa = spec(fa, r), wb = spec(fb, r);
+                const C wa = fa[F::sw(k)], wb = fb[F::sw(k)];
                 C u = csub(cmul(wa, A), cmul(wb, B));
                 // kx >= L/2 and kx = 0: the reference's form (see above); the
                 // line's own symbol flips sign at -k except at kx = L/2
@@ -924,6 +896,17 @@ inline cudaError_t launch_row_fused_shape(int sh, int L, const RowFusedArgs& a, 
     return launch_row_fused_len<T, SH_ANY, ROT>(L, a, ncomp, s);
 }
 
+// CTAs per SM the real-side columns ask the compiler for (FLB_COLREAL_PER_SM
+// > 0: threads per SM, else the column passes' figure)
+#ifndef FLB_COLREAL_PER_SM
+#define FLB_COLREAL_PER_SM 0
+#endif
+template <int THREADS>
+struct ColRealOcc {
+    static constexpr int blocks =
+        FLB_COLREAL_PER_SM > 0 ? (FLB_COLREAL_PER_SM / THREADS > 0 ? FLB_COLREAL_PER_SM / THREADS : 1) : Occ<THREADS>::blocks;
+};
+
 // ---------------------------------------------------------------- columns, real side
 // r2c (C2R = false): real column of nin values (zero beyond) -> X[0..L/2];
 // SH: loaded part.  c2r (C2R = true): X[0..L/2] -> real column, the upper half
@@ -932,7 +915,7 @@ inline cudaError_t launch_row_fused_shape(int sh, int L, const RowFusedArgs& a, 
 // RT: type of the real side (the working precision, or the user's doubles
 // when the pass is the first or last of a solve).
 template <typename T, typename RT, int L, int R1, int TX, bool C2R, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1)>::blocks)) col_real_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), ColRealOcc<TX * (L / R1)>::blocks) col_real_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     constexpr int P = F::P;
@@ -1036,7 +1019,7 @@ struct CPair {
 };
 
 template <typename T, typename RT, int L, int R1, int TXP, bool C2R, int SH>
-__global__ void __launch_bounds__(TXP * (L / R1), (Occ<TXP * (L / R1)>::blocks)) col_real_pair_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TXP * (L / R1), ColRealOcc<TXP * (L / R1)>::blocks) col_real_pair_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     using R2 = typename Vec2<RT>::V;
