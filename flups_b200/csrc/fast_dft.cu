@@ -107,12 +107,22 @@ bool fast_r2r_supported(int M) {
     return false;
 }
 
-int fast_dct_family(int kind, int n, int M) {
-    if (M != 2 * n) return 0;
+#ifndef FLB_DCT1_HALF
+#define FLB_DCT1_HALF 1
+#endif
+static bool dct_len_ok(int n) {
     switch (n) {
-        case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: break;
-        default: return 0;
+        case 64: case 96: case 128: case 192: case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: return true;
     }
+    return false;
+}
+
+int fast_dct_length(int kind, int n, int M) { return fast_dct_family(kind, n, M) == 1 ? M : n; }
+
+int fast_dct_family(int kind, int n, int M) {
+    // DCT-I / DST-I: the M-point real DFT of the even / odd extension
+    if ((kind == LK_DCT1 && M == 2 * (n - 1)) || (kind == LK_DST1 && M == 2 * (n + 1))) return (FLB_DCT1_HALF && dct_len_ok(M)) ? 1 : 0;
+    if (M != 2 * n || !dct_len_ok(n)) return 0;
     switch (kind) {
         case LK_DCT2: case LK_DST2: return 2;
         case LK_DCT3: case LK_DST3: return 3;
@@ -123,6 +133,7 @@ int fast_dct_family(int kind, int n, int M) {
 
 cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s) {
     switch (fast_dct_family(a.kind, a.n, M)) {
+        case 1: return launch_dct1_units(f64, a.in_f64, a.out_f64, M, a, ncomp, s);
         case 2: return launch_dct2_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);
         case 3: return launch_dct3_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);
         case 4: return launch_dct4_units(f64, a.in_f64, a.out_f64, a.n, a, ncomp, s);

@@ -95,6 +95,8 @@ struct RowArgs {
     int n;                  // FFTW size n_in
     int nstore;             // outputs written (before post-processing)
     int postpro, nfftw;     // PostPro bits and the index PP_ENFORCE_PERIOD copies from 0
+    int fi, fo;             // first input / output element of the transform in its row (half-length DCT kinds)
+    int ilast;              // the row element PP_NULL_LAST sets to zero (the output line's last)
     const void* tw2;        // W_{2M}^q, q < 2M (pre/post twiddles of the r2r kinds)
     Prefetch pf;            // r2c / c2r rows
 };
@@ -204,10 +206,13 @@ cudaError_t launch_fast_row(int f64, int c2r, int L, const RowArgs& a, int ncomp
 // r2r rows (DCT / DST I-IV) through an M-point complex register DFT
 bool fast_r2r_supported(int M);
 // DCT / DST II-IV rows of even length n (M = 2n) that run through one
-// n/2-point register DFT instead: the family (2, 3 or 4), else 0.  Their
-// tables: tw = W_n^q (q < n), tws = the stage table of the n/2-point DFT,
-// tw2 = W_2M^q as for the M-point kernel.
+// n/2-point register DFT instead: the family (2, 3 or 4); DCT-I / DST-I rows
+// (M = 2(n - 1) / 2(n + 1)) through one M/2-point register DFT: family 1;
+// else 0.  Their tables, with N = fast_dct_length (n, or M for family 1):
+// tw = W_N^q (q < N), tws = the stage table of the N/2-point DFT, tw2 =
+// W_2M^q as for the M-point kernel.
 int fast_dct_family(int kind, int n, int M);
+int fast_dct_length(int kind, int n, int M);
 // launches the half-length kernel when fast_dct_family(a.kind, a.n, M) != 0
 cudaError_t launch_fast_r2r(int f64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
 // column r2c (c2r = 0: real in, X[0..L/2] out) and c2r (c2r = 1)

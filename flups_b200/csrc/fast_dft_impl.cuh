@@ -781,31 +781,32 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
     {
         const C* fa = line_of(ga);
         const C* fb = line_of(gb);
-        auto curl = [&](auto mode) {
-            constexpr int VARY = decltype(mode)::value;
+        {
+            // one code path for the three components of the triple (which
+            // symbol varies along the row is a per-warp value): three unrolled
+            // variants, one per component, missed the instruction cache
+            // (fused rows 3.05 -> 2.94 ms at 384^3)
+            const bool v1 = vary == 1, v2 = vary == 2;
+            const C* kt = ktab ? ktab : K;
 #pragma unroll
             for (int r = 0; r < R1; ++r) {
                 const int k = p + P * r;
-                const C A = (VARY == 1) ? __ldg(ktab + k) : ka;
-                const C B = (VARY == 2) ? __ldg(ktab + k) : kb;
+                const C kv = vary ? __ldg(kt + k) : mkc((T)0, (T)0);
+                const C A = v1 ? kv : ka;
+                const C B = v2 ? kv : kb;
                 const C wa = fa[F::sw(k)], wb = fb[F::sw(k)];
                 C u = csub(cmul(wa, A), cmul(wb, B));
-                // kx >= L/2 and kx = 0: the reference's form (see above); the
-                // line's own symbol flips sign at -k except at kx = L/2
                 if (r >= R1 / 2 || (r == 0 && p == 0)) {
                     const bool edge = (p == 0) && (r == 0 || r == R1 / 2);
                     const T lsign = (p == 0 && r == R1 / 2) ? (T)1 : (T)-1;
-                    const T qa = (VARY == 1) ? lsign : sa, qb = (VARY == 2) ? lsign : sb;
+                    const T qa = v1 ? lsign : sa, qb = v2 ? lsign : sb;
                     const C ca = cconj(A), cb = cconj(B);
                     const C q = csub(cmul(wa, mkc(qa * ca.x, qa * ca.y)), cmul(wb, mkc(qb * cb.x, qb * cb.y)));
                     u = edge ? mkc((T)0.5 * (u.x + q.x), (T)0.5 * (u.y + q.y)) : q;
                 }
                 v[r] = cscale(u, r < R1 / 2 ? gs[k] : gs[L - k]);
             }
-        };
-        if (vary == 1) curl(std::integral_constant<int, 1>{});
-        else if (vary == 2) curl(std::integral_constant<int, 2>{});
-        else curl(std::integral_constant<int, 0>{});
+        }
     }
     // the triple has read every spectrum before the inverse DFT reuses the lines
     asm volatile("bar.sync %0, 96;" ::"r"(1 + tri) : "memory");
@@ -896,15 +897,19 @@ inline cudaError_t launch_row_fused_shape(int sh, int L, const RowFusedArgs& a, 
     return launch_row_fused_len<T, SH_ANY, ROT>(L, a, ncomp, s);
 }
 
-// CTAs per SM the real-side columns ask the compiler for (FLB_COLREAL_PER_SM
-// > 0: threads per SM, else the column passes' figure)
+// CTAs per SM the real-side columns ask the compiler for: three for FP32
+// real-to-complex lines of a first radix up to 24 (80 registers; 384^3 ROT z
+// forward 0.568 -> 0.514 ms; the complex-to-real lines and the radix-32
+// lines were slower so), else the column passes' figure;
+// FLB_COLREAL_PER_SM > 0 sets threads per SM for all of them
 #ifndef FLB_COLREAL_PER_SM
 #define FLB_COLREAL_PER_SM 0
 #endif
-template <int THREADS>
+template <typename T, int R1, bool C2R, int THREADS>
 struct ColRealOcc {
+    static constexpr int dflt = (sizeof(T) == 4 && !C2R && R1 <= 24 && THREADS == 256) ? 3 : Occ<THREADS>::blocks;
     static constexpr int blocks =
-        FLB_COLREAL_PER_SM > 0 ? (FLB_COLREAL_PER_SM / THREADS > 0 ? FLB_COLREAL_PER_SM / THREADS : 1) : Occ<THREADS>::blocks;
+        FLB_COLREAL_PER_SM > 0 ? (FLB_COLREAL_PER_SM / THREADS > 0 ? FLB_COLREAL_PER_SM / THREADS : 1) : dflt;
 };
 
 // ---------------------------------------------------------------- columns, real side
@@ -915,7 +920,7 @@ struct ColRealOcc {
 // RT: type of the real side (the working precision, or the user's doubles
 // when the pass is the first or last of a solve).
 template <typename T, typename RT, int L, int R1, int TX, bool C2R, int SH>
-__global__ void __launch_bounds__(TX * (L / R1), ColRealOcc<TX * (L / R1)>::blocks) col_real_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TX * (L / R1), ColRealOcc<T, R1, C2R, TX * (L / R1)>::blocks) col_real_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     constexpr int P = F::P;
@@ -1019,7 +1024,7 @@ struct CPair {
 };
 
 template <typename T, typename RT, int L, int R1, int TXP, bool C2R, int SH>
-__global__ void __launch_bounds__(TXP * (L / R1), ColRealOcc<TXP * (L / R1)>::blocks) col_real_pair_kernel(const ColArgs a) {
+__global__ void __launch_bounds__(TXP * (L / R1), ColRealOcc<T, R1, C2R, TXP * (L / R1)>::blocks) col_real_pair_kernel(const ColArgs a) {
     using F = RegFFT<T, L, R1>;
     using C = typename CT<T>::C;
     using R2 = typename Vec2<RT>::V;
@@ -1317,7 +1322,7 @@ __global__ void __launch_bounds__(TR * (M / R1), (Occ<TR * (M / R1)>::blocks)) r
         if (i >= a.nstore) continue;
         T y;
         if (first && i == 0) y = z;
-        else if (last && i == a.nstore - 1) y = z;
+        else if (last && i == a.ilast) y = z;
         else if (period && !first && !last && i == a.nfftw) y = value(0);
         else y = value(i);
         dst[i] = (OT)y;
@@ -1346,8 +1351,8 @@ __global__ void __launch_bounds__(TR * (M / R1), (Occ<TR * (M / R1)>::blocks)) r
 // shared memory when they take at most 8 KB
 template <typename T, int FAM, int LH>
 struct DctW4 {
-    static constexpr int USED = (FAM == 4) ? 2 * LH : LH + 1;
-    static constexpr bool SM = USED * (int)sizeof(typename CT<T>::C) <= 8192;
+    static constexpr int USED = (FAM == 4) ? 2 * LH : (FAM == 1 ? 0 : LH + 1);
+    static constexpr bool SM = USED > 0 && USED * (int)sizeof(typename CT<T>::C) <= 8192;
     static constexpr int N = SM ? USED : 0;
 };
 
@@ -1380,7 +1385,9 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
     const int comp = blockIdx.y;
     const bool valid = row < a.nrows;
     const int i1 = valid ? row % a.n1 : 0, i2 = valid ? row / a.n1 : 0;
-    const IT* src = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
+    // src0: the row; src: the transform's first input (fi into the row)
+    const IT* src0 = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
+    const IT* src = src0 + a.fi;
     C* line = sm + rr * F::SC;
     T* lr = reinterpret_cast<T*>(line);
     const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
@@ -1394,8 +1401,10 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
         w4 = w4s;
     }
     cp_async_commit();
-    const bool dst = (a.kind == LK_DST2 || a.kind == LK_DST3 || a.kind == LK_DST4);
-    const int nld = valid ? (a.nin < N ? a.nin : N) : 0;
+    const bool dst = (a.kind == LK_DST1 || a.kind == LK_DST2 || a.kind == LK_DST3 || a.kind == LK_DST4);
+    // inputs the transform reads: n (DCT-I n = LH + 1, DST-I n = LH - 1), else up to N
+    const int ntr = (FAM == 1) ? a.n : N;
+    const int nld = valid ? (a.nin - a.fi < ntr ? a.nin - a.fi : ntr) : 0;
     const T z = (T)0;
     // real m of the packed line: z_j = (r_{2j}, r_{2j+1}) at line[sw(j)]
     auto slot = [](int m) { return 2 * F::sw(m >> 1) + (m & 1); };
@@ -1433,14 +1442,38 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
             }
         }
     };
-    // rows that hold all N inputs load them without a test per element
-    if (nld >= N) stage(std::true_type{});
-    else stage(std::false_type{});
+    if constexpr (FAM == 1) {
+        // the 2 LH-point real extension z of the row, packed: DCT-I z_j = x_j for
+        // j <= LH, z_{2LH-j} = x_j; DST-I z_{j+1} = x_j, z_{2LH-1-j} = -x_j,
+        // z_0 = z_LH = 0.  Lane p loads x_i, i = p + P r (i < LH), lane 0 also
+        // i = LH; every x_i lands in its one or two places.
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int i = p + P * r;
+            const T u = (i < nld) ? (T)src[i] : z;
+            if (dst) {
+                lr[slot(i + 1)] = u;
+                lr[slot(N - 1 - i)] = -u;
+            } else {
+                lr[slot(i)] = u;
+                if (i > 0) lr[slot(N - i)] = u;
+            }
+        }
+        if (p == 0) {
+            const T u = (!dst && LH < nld) ? (T)src[LH] : z;
+            lr[slot(LH)] = u;  // DCT-I: x_LH; DST-I: z_LH = 0
+            if (dst) lr[slot(0)] = z;
+        }
+    } else {
+        // rows that hold all N inputs load them without a test per element
+        if (nld >= N) stage(std::true_type{});
+        else stage(std::false_type{});
+    }
     cp_async_wait<0>();
     __syncthreads();
     const C* wn = WSM ? wsm : reinterpret_cast<const C*>(a.tw);
     C v[R1];
-    if constexpr (FAM == 2) {
+    if constexpr (FAM == 1 || FAM == 2) {
 #pragma unroll
         for (int r = 0; r < R1; ++r) v[r] = line[F::sw(p + P * r)];
     } else if constexpr (FAM == 4) {
@@ -1502,6 +1535,32 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
             const C u = cmul(v[r], w4[2 * k]);
             line[F::sw(k)] = mkc((T)2 * u.x, (T)-2 * u.y);  // (Y_{2k}, Y_{n-1-2k})
         }
+    } else if constexpr (FAM == 1) {
+        // the N-point real DFT Z of z from the packed LH-point DFT C:
+        // Z_k = E_k + W_N^k O_k, E_k = (C_k + conj C_{LH-k}) / 2,
+        // O_k = (C_k - conj C_{LH-k}) / 2i (C_LH = C_0); DCT-I Y_k = Re Z_k
+        // (k <= LH, Z_LH = Re C_0 - Im C_0), DST-I Y_{k-1} = -Im Z_k (0 < k < LH).
+        // The real outputs are then laid out in row order over the line.
+        __syncthreads();
+        T y[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            const C zk = v[r];
+            const C zm = cconj(line[F::sw(k == 0 ? 0 : LH - k)]);
+            const C e = cadd(zk, zm);
+            const C w = cmul(wn[k], csub(zk, zm));
+            y[r] = dst ? (T)-0.5 * (e.y - w.x) : (T)0.5 * (e.x + w.y);
+        }
+        const T ylh = v[0].x - v[0].y;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            if (!dst) lr[k] = y[r];
+            else if (k > 0) lr[k - 1] = y[r];
+        }
+        if (p == 0 && !dst) lr[LH] = ylh;
     }
     __syncthreads();
     if (!valid) return;
@@ -1513,19 +1572,26 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
         } else if constexpr (FAM == 3) {
             const T y = lr[slot((i & 1) ? N - 1 - (i >> 1) : (i >> 1))];
             return (dst && (i & 1)) ? -y : y;
+        } else if constexpr (FAM == 1) {
+            return lr[i];
         } else {
             const T y = (i & 1) ? line[F::sw((N - 1 - i) >> 1)].y : line[F::sw(i >> 1)].x;
             return (dst && (i & 1)) ? -y : y;
         }
     };
     const bool first = a.postpro & PP_NULL_FIRST, last = a.postpro & PP_NULL_LAST, period = a.postpro & PP_ENFORCE_PERIOD;
+    // row element i: transform output i - fo, else the row's input stays
+    auto outv = [&](int i) -> T {
+        const int k = i - a.fo;
+        if (k < 0 || k >= ntr) return (i < a.nin) ? (T)src0[i] : z;
+        return value(k);
+    };
     auto store = [&](int i) {
         T y;
         if (first && i == 0) y = z;
-        else if (last && i == a.nstore - 1) y = z;
-        else if (period && !first && !last && i == a.nfftw) y = value(0);
-        else if (i >= N) y = (i < a.nin) ? (T)src[i] : z;
-        else y = value(i);
+        else if (last && i == a.ilast) y = z;
+        else if (period && !first && !last && i == a.nfftw) y = outv(0);
+        else y = outv(i);
         out[i] = (OT)y;
     };
     if constexpr (FAM == 3) {
@@ -1628,6 +1694,8 @@ cudaError_t launch_colreal_f32(int c2r, int sh, int L, const ColArgs& a, int nco
 // FP32 columns whose real side is the user's doubles
 cudaError_t launch_colreal_f32u(int c2r, int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_r2r_units(int f64, int in64, int out64, int M, const RowArgs& a, int ncomp, cudaStream_t s);
+// n: the real DFT length of the extension (M)
+cudaError_t launch_dct1_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_dct2_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_dct3_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);
 cudaError_t launch_dct4_units(int f64, int in64, int out64, int n, const RowArgs& a, int ncomp, cudaStream_t s);

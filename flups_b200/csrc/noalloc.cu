@@ -165,8 +165,9 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             const LineSpec& sp = A.st[0].spec[0];
             slot_for(2 * A.st[0].M, 0);
             if (fast_dct_family(sp.kind, sp.n_in, A.st[0].M)) {
-                slot_for(sp.n_in, 0);
-                slot_for(sp.n_in / 2, fast_radix1_dct(sp.n_in / 2, f64 ? 1 : 0));
+                const int nt = fast_dct_length(sp.kind, sp.n_in, A.st[0].M);
+                slot_for(nt, 0);
+                slot_for(nt / 2, fast_radix1_dct(nt / 2, f64 ? 1 : 0));
             } else {
                 slot_for(A.st[0].M, r1_of(A.st[0].M));
             }
@@ -223,8 +224,9 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                 } else if (kinds[i] == 4) {
                     r.tw2 = tw_of(2 * L, 0);
                     if (fast_dct_family(r.kind, r.n, L)) {
-                        r.tw = tw_of(r.n, 0);
-                        r.tws = tw_of(r.n / 2, fast_radix1_dct(r.n / 2, f64 ? 1 : 0));
+                        const int nt = fast_dct_length(r.kind, r.n, L);
+                        r.tw = tw_of(nt, 0);
+                        r.tws = tw_of(nt / 2, fast_radix1_dct(nt / 2, f64 ? 1 : 0));
                     } else {
                         r.tws = tw_of(L, r1_of(L));
                     }

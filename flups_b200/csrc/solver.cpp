@@ -574,10 +574,15 @@ int Solver::fast_kind(const PassArgs& A, bool f64, bool in_f64, bool out_f64) co
         // r2r rows (DCT / DST I-IV): the post-processing is done by the kernel
         if (k0 >= LK_DCT1 && k0 <= LK_DST4) {
             if (A.fused || A.axis != 0) return 0;
-            if (!fast_r2r_supported(S0.M) && !fast_dct_family(k0, S0.spec[0].n_in, S0.M)) return 0;
+            const bool half = fast_dct_family(k0, S0.spec[0].n_in, S0.M) != 0;
+            if (!fast_r2r_supported(S0.M) && !half) return 0;
+            // the half-length kernels place the transform at fi / fo in its row
+            // (node-centred DST-I: the boundary values stay outside); the
+            // M-point kernel does not
+            if (!half && (S0.spec[0].fi != 0 || S0.spec[0].fo != 0)) return 0;
             for (int c = 0; c < A.lda; ++c) {
                 const LineSpec& sp = S0.spec[c];
-                if (sp.kind != k0 || sp.n_in != S0.spec[0].n_in || sp.fi != 0 || sp.fo != 0 ||
+                if (sp.kind != k0 || sp.n_in != S0.spec[0].n_in || sp.fi != S0.spec[0].fi || sp.fo != S0.spec[0].fo ||
                     sp.postpro != S0.spec[0].postpro || sp.nfftw != S0.spec[0].nfftw)
                     return 0;
             }
@@ -707,6 +712,9 @@ void Solver::fast_args(const PassArgs& A, int kind, bool in_f64, bool out_f64, C
     r.nstore = S0.n_store;
     r.postpro = S0.spec[0].postpro;
     r.nfftw = S0.spec[0].nfftw;
+    r.fi = S0.spec[0].fi;
+    r.fo = S0.spec[0].fo;
+    r.ilast = S0.n_o - 1;
     r.in_s1 = A.in_str[1];
     r.in_s2 = A.in_str[2];
     r.in_cstr = A.in_cstr;
@@ -764,8 +772,9 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     if (kind == 4) {
         r.tw2 = twiddle(L, f64);
         if (fast_dct_family(r.kind, r.n, L)) {
-            r.tw = twiddle_plain(r.n, f64);
-            r.tws = stage_table(r.n / 2, f64, fast_radix1_dct(r.n / 2, f64 ? 1 : 0));
+            const int nt = fast_dct_length(r.kind, r.n, L);
+            r.tw = twiddle_plain(nt, f64);
+            r.tws = stage_table(nt / 2, f64, fast_radix1_dct(nt / 2, f64 ? 1 : 0));
         } else {
             r.tws = stage_table(L, f64);
         }
