@@ -146,8 +146,17 @@ __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
 #ifndef FLB_ROWROT_R48
 #define FLB_ROWROT_R48 1
 #endif
+// the fused rows (row_fused_kernel, row_rot_kernel) of FP64 3 x 2^k lines:
+// a first radix of 24 (P = n / 24 lanes per row, so lines up to 768 points
+// fit one warp and the x-last order applies), else the fused passes' radix
+#ifndef FLB_ROWF64_R24
+#define FLB_ROWF64_R24 1
+#endif
+__host__ __device__ constexpr int fast_radix1_rowfused(int n, int f64) {
+    return (FLB_ROWF64_R24 && f64 && n % 3 == 0 && n % 24 == 0 && n / 24 <= 32 && n / 24 >= 2) ? 24 : fast_radix1_mode(n, f64, 2);
+}
 __host__ __device__ constexpr int fast_radix1_rowrot(int n, int f64) {
-    return (FLB_ROWROT_R48 && fast_radix48(n, f64)) ? 48 : fast_radix1_mode(n, f64, 2);
+    return (FLB_ROWROT_R48 && fast_radix48(n, f64)) ? 48 : fast_radix1_rowfused(n, f64);
 }
 // the half-length DCT / DST rows (row_dct_kernel): the LH-point DFT's first
 // radix.  FP32 power-of-two lines up to 256 points take 16 (16 complex values

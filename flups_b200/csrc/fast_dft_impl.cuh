@@ -843,12 +843,12 @@ inline cudaError_t launch_row_rot_t(const RowFusedArgs& a, int ncomp, cudaStream
 // lines of first radix R1 whose P = L / R1 threads fit in one warp
 __host__ __device__ constexpr bool fast_rowfused_len(int L, int f64) {
     return (L == 48 || L == 64 || L == 96 || L == 128 || L == 192 || L == 256 || L == 384 || L == 512 || L == 768 || L == 1024) &&
-           L / fast_radix1_mode(L, f64, 2) <= 32;
+           L / fast_radix1_rowfused(L, f64) <= 32;
 }
 
 template <typename T, int L, int WARPS, int SH>
 inline cudaError_t launch_row_fused_t(const RowFusedArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = fast_radix1_mode(L, sizeof(T) == 8, 2);
+    constexpr int R1 = fast_radix1_rowfused(L, sizeof(T) == 8);
     using F = RegFFT<T, L, R1, true, true, true>;
     constexpr int LPW = 32 / F::P;
     constexpr size_t smem = (size_t)WARPS * LPW * (F::SC * sizeof(typename CT<T>::C) + RowFusedTile<T, L>::GP * sizeof(T));

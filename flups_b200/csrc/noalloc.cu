@@ -160,7 +160,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
             slot_for(A.st[0].M, r1_of(A.st[0].M));
         } else if (kinds[i] == 5) {
             const int M = A.st[0].M;
-            slot_for(M, A.mult.mode == 2 ? fast_radix1_rowrot(M, f64 ? 1 : 0) : fast_radix1_mode(M, f64 ? 1 : 0, 2));
+            slot_for(M, A.mult.mode == 2 ? fast_radix1_rowrot(M, f64 ? 1 : 0) : fast_radix1_rowfused(M, f64 ? 1 : 0));
         } else if (kinds[i] == 4) {
             const LineSpec& sp = A.st[0].spec[0];
             slot_for(2 * A.st[0].M, 0);
@@ -207,7 +207,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                 RowFusedArgs f;
                 s->rowfused_args(A, f);
                 const int L = A.st[0].M;
-                f.tws = tw_of(L, A.mult.mode == 2 ? fast_radix1_rowrot(L, f64 ? 1 : 0) : fast_radix1_mode(L, f64 ? 1 : 0, 2));
+                f.tws = tw_of(L, A.mult.mode == 2 ? fast_radix1_rowrot(L, f64 ? 1 : 0) : fast_radix1_rowfused(L, f64 ? 1 : 0));
                 if (go) e = launch_fast_rowfused(f64 ? 1 : 0, A.mult.mode == 2, L, f, A.ncomp, st);
             } else {
                 const int L = A.st[0].M;

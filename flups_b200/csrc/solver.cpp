@@ -761,7 +761,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
     if (kind == 5) {
         RowFusedArgs f;
         rowfused_args(A, f);
-        f.tws = stage_table(L, f64, A.mult.mode == 2 ? fast_radix1_rowrot(L, f64 ? 1 : 0) : fast_radix1_mode(L, f64 ? 1 : 0, 2));
+        f.tws = stage_table(L, f64, A.mult.mode == 2 ? fast_radix1_rowrot(L, f64 ? 1 : 0) : fast_radix1_rowfused(L, f64 ? 1 : 0));
         check_cuda(launch_fast_rowfused(f64 ? 1 : 0, A.mult.mode == 2, L, f, A.ncomp, stream), "fused row launch");
         return;
     }

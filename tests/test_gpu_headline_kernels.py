@@ -39,6 +39,10 @@ CASES = [
     ("rows3072_1536x16x16", [1536, 16, 16], UNB3, CELL_CENTER, CHAT_2, 3072, 0),
     ("cols1536_16x768x16", [16, 768, 16], UNB3, CELL_CENTER, CHAT_2, 1536, 1),
     ("fused1536_16x16x768", [16, 16, 768], UNB3, CELL_CENTER, CHAT_2, 1536, 2),
+    # 768- and 384-point x rows: with device arrays the fused rows of the
+    # x-last order (FP64 3 x 2^k rows run a first radix of 24)
+    ("xrows768_384x24x24", [384, 24, 24], UNB3, CELL_CENTER, CHAT_2, 768, 0),
+    ("xrows384_192x24x24", [192, 24, 24], UNB3, CELL_CENTER, LGF_2, 384, 0),
     ("node513_dct_rows_eo_per_unb", [513, 33, 33], EO_PER_UNB, NODE_CENTER, HEJ_4, 1024, 0),
     # DCT-I / DST-I rows (node-centred EVEN/EVEN, ODD/ODD): the real DFT of the
     # extension through a register DFT of half its length
