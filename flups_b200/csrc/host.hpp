@@ -246,6 +246,7 @@ struct Solver {
     // the two sets for the duration of a solve; the folded Green's spectrum
     // is the same array in both orders.
     bool has_xlast = false;
+    bool xlast_mixed = false;  // the x-last plans include a periodic direction
     bool xlast_on = true;                 // flups_b200_set_xlast
     bool xlast_active = false;
     flb::DirPlan xfwd[3], xbwd[3], xdif[3];

@@ -145,8 +145,14 @@ Solver::Solver(Topology* t, FLUPS_BoundaryType* bcin[3][2], const double hin[3],
 // order z, y, x, so z becomes the real-to-complex direction.
 void Solver::build_xlast() {
     if (ndim != 3) return;
-    for (int ip = 0; ip < 3; ++ip)
-        if (fwd[ip].type != UNBUNB) return;
+    // every direction unbounded or periodic: z, y, x is then a valid order of
+    // the same transforms (the Green's spectrum is even in each direction and
+    // folds to the same extents in both orders; compute_green checks it)
+    xlast_mixed = false;
+    for (int ip = 0; ip < 3; ++ip) {
+        if (fwd[ip].type == PERPER) xlast_mixed = true;
+        else if (fwd[ip].type != UNBUNB) return;
+    }
     const int order[3] = {2, 1, 0};
     for (int k = 0; k < 3; ++k) {
         const int d = order[k];
@@ -200,7 +206,11 @@ void Solver::plan_xlast() {
     if (!has_xlast) return;
     for (int t = 0; t < 2; ++t) {
         const int type = t ? ROT : STD;
-        if (type == ROT && (lda != 3 || !have_diff)) continue;
+        // ROT keeps the reference's order when a direction is periodic: its
+        // curl's Nyquist treatment in the fused rows reproduces the spectrum
+        // of the reference's real-to-complex direction for the all-unbounded
+        // order only
+        if (type == ROT && (lda != 3 || !have_diff || xlast_mixed)) continue;
         swap_order();
         const bool keep = dry;
         dry = true;
@@ -1186,8 +1196,9 @@ void Solver::compute_green() {
         for (int d = 0; d < 3; ++d) xgfold_M[d] = 0;
         for (int ip = 0; ip < ndim; ++ip) {
             const DirPlan& p = xfwd[ip];
-            const int fn = (p.type == UNBUNB && !p.isr2c) ? p.n_in[0] / 2 + 1 : xst[ndim].n[p.dim];
-            if (p.type == UNBUNB && !p.isr2c) xgfold_M[p.dim] = p.n_in[0];
+            const bool fold = (p.type == UNBUNB || p.type == PERPER) && !p.isr2c;
+            const int fn = fold ? p.n_in[0] / 2 + 1 : xst[ndim].n[p.dim];
+            if (fold) xgfold_M[p.dim] = p.n_in[0];
             if (fn != gfold_n[p.dim]) has_xlast = false;
         }
     }

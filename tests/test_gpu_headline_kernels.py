@@ -174,3 +174,40 @@ def test_full_256_cube_fp64_matches_oracle():
             _check_fast(plan, 2 * n, axis)
         assert plan["xlast"] == (1 if device else 0)
         assert rel_l2(got, ref) <= 1e-12
+
+
+# grids whose directions are all unbounded or periodic (line lengths the
+# register DFTs take in every direction): device arrays run the x-last order
+# for STD solves (z first, the fused pass along x rows), ROT keeps the
+# reference's order there
+PPU = [[[3], [3]], [[3], [3]], [[4], [4]]]
+UPU = [[[4], [4]], [[3], [3]], [[4], [4]]]
+PUP = [[[3], [3]], [[4], [4]], [[3], [3]]]
+MIXED = [
+    ("per_per_unb_64x48x32", [64, 48, 32], PPU, HEJ_4),
+    ("unb_per_unb_48x64x32", [48, 64, 32], UPU, LGF_2),
+    ("per_unb_per_64x32x48", [64, 32, 48], PUP, CHAT_2),
+]
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("name,nglob,bcv,kernel", MIXED, ids=[c[0] for c in MIXED])
+def test_mixed_periodic_unbounded_xlast(name, nglob, bcv, kernel, precision, tol):
+    rhs = _rhs(nglob)
+    got, plan = _solve(nglob, 1, bcv, CELL_CENTER, kernel, precision, rhs, device=True)
+    assert plan["xlast"] == 1
+    fused = [p for p in plan["passes"] if p["name"] == "fused"]
+    assert fused[0]["axis"] == 0 and fused[0]["fast"] == 5
+    ref = _oracle(name, nglob, 1, bcv, CELL_CENTER, kernel, rhs)
+    assert rel_l2(got, ref) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
+def test_mixed_rot_keeps_reference_order(precision, tol):
+    nglob = [32, 32, 48]
+    bcv = [[[3] * 3, [3] * 3], [[3] * 3, [3] * 3], [[4] * 3, [4] * 3]]
+    rhs = _rhs(nglob, lda=3, seed=29)
+    got, plan = _solve(nglob, 3, bcv, CELL_CENTER, LGF_4, precision, rhs, type_=1, odiff=1, device=True)
+    assert plan["xlast"] == 0
+    ref = _oracle("rot_per_per_unb", nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
+    assert rel_l2(got, ref) <= tol
