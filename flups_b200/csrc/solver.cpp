@@ -206,11 +206,11 @@ void Solver::plan_xlast() {
     if (!has_xlast) return;
     for (int t = 0; t < 2; ++t) {
         const int type = t ? ROT : STD;
-        // ROT keeps the reference's order when a direction is periodic: its
-        // curl's Nyquist treatment in the fused rows reproduces the spectrum
-        // of the reference's real-to-complex direction for the all-unbounded
-        // order only
-        if (type == ROT && (lda != 3 || !have_diff || xlast_mixed)) continue;
+        // ROT: the fused rows' Nyquist treatment reproduces the spectrum of a
+        // reference order whose real-to-complex direction is x; with a
+        // periodic direction that holds when x is the reference's first
+        // direction (periodic x), else the reference's order stays
+        if (type == ROT && (lda != 3 || !have_diff || (xlast_mixed && fwd[0].dim != 0))) continue;
         swap_order();
         const bool keep = dry;
         dry = true;

@@ -97,8 +97,8 @@ void flups_b200_set_overlap(struct Solver* s, int on);
 void flups_b200_set_prefetch(struct Solver* s, int on);
 
 /* Pass order of 3-D solves of device arrays whose directions are all
- * unbounded or periodic (ROT: all unbounded) (1 = x last, the default; 0 =
- * the reference's order).  With x last, z is the
+ * unbounded or periodic (ROT: when x is the reference's first direction)
+ * (1 = x last, the default; 0 = the reference's order).  With x last, z is the
  * real-to-complex direction and the last pass -- forward DFT, Green's
  * multiply, inverse DFT -- runs along contiguous x rows, one warp per row
  * (1.28 against 2.04 ms for that pass at 512^3 FP32).  The result equals the

@@ -178,8 +178,7 @@ def test_full_256_cube_fp64_matches_oracle():
 
 # grids whose directions are all unbounded or periodic (line lengths the
 # register DFTs take in every direction): device arrays run the x-last order
-# for STD solves (z first, the fused pass along x rows), ROT keeps the
-# reference's order there
+# (z first, the fused pass along x rows)
 PPU = [[[3], [3]], [[3], [3]], [[4], [4]]]
 UPU = [[[4], [4]], [[3], [3]], [[4], [4]]]
 PUP = [[[3], [3]], [[4], [4]], [[3], [3]]]
@@ -202,12 +201,24 @@ def test_mixed_periodic_unbounded_xlast(name, nglob, bcv, kernel, precision, tol
     assert rel_l2(got, ref) <= tol
 
 
+def _bc3(codes):
+    return [[[c[0]] * 3, [c[1]] * 3] for c in codes]
+
+
+# ROT with periodic directions: the x-last order when the reference's first
+# (real-to-complex) direction is x (periodic x), else the reference's order
+ROT_MIXED = [
+    ("rot_per_per_unb_64x48x32", [64, 48, 32], _bc3([(3, 3), (3, 3), (4, 4)]), 1),
+    ("rot_per_unb_per_48x32x64", [48, 32, 64], _bc3([(3, 3), (4, 4), (3, 3)]), 1),
+    ("rot_unb_per_unb_24x48x32", [24, 48, 32], _bc3([(4, 4), (3, 3), (4, 4)]), 0),
+]
+
+
 @pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-6)], ids=["fp64", "fp32"])
-def test_mixed_rot_keeps_reference_order(precision, tol):
-    nglob = [32, 32, 48]
-    bcv = [[[3] * 3, [3] * 3], [[3] * 3, [3] * 3], [[4] * 3, [4] * 3]]
+@pytest.mark.parametrize("name,nglob,bcv,xlast", ROT_MIXED, ids=[c[0] for c in ROT_MIXED])
+def test_mixed_rot(name, nglob, bcv, xlast, precision, tol):
     rhs = _rhs(nglob, lda=3, seed=29)
     got, plan = _solve(nglob, 3, bcv, CELL_CENTER, LGF_4, precision, rhs, type_=1, odiff=1, device=True)
-    assert plan["xlast"] == 0
-    ref = _oracle("rot_per_per_unb", nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
+    assert plan["xlast"] == xlast
+    ref = _oracle(name, nglob, 3, bcv, CELL_CENTER, LGF_4, rhs, type_=1, odiff=1)
     assert rel_l2(got, ref) <= tol
