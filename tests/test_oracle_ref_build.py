@@ -12,8 +12,7 @@ or a CPU baseline:
    whole solution fields, including cases no golden covers (the 1-unbounded
    LGF_4/6/8 and MEHR kernels, finite-difference ROT orders).
 
-CPU only; skipped where the reference tree or g++ is absent (the builds
-come from /root/reference here).
+CPU only; skipped where the reference tree or g++ is absent.
 """
 import ctypes
 import json
