@@ -788,6 +788,9 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
             // (fused rows 3.05 -> 2.94 ms at 384^3)
             const bool v1 = vary == 1, v2 = vary == 2;
             const C* kt = ktab ? ktab : K;
+            // the Q form's symbols: the constant ones (sign times conjugate)
+            // once per lane; the varying one is -conj(kv), conj(kv) at kx = N
+            const C qka = mkc(sa * ka.x, -sa * ka.y), qkb = mkc(sb * kb.x, -sb * kb.y);
 #pragma unroll
             for (int r = 0; r < R1; ++r) {
                 const int k = p + P * r;
@@ -798,10 +801,8 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
                 C u = csub(cmul(wa, A), cmul(wb, B));
                 if (r >= R1 / 2 || (r == 0 && p == 0)) {
                     const bool edge = (p == 0) && (r == 0 || r == R1 / 2);
-                    const T lsign = (p == 0 && r == R1 / 2) ? (T)1 : (T)-1;
-                    const T qa = v1 ? lsign : sa, qb = v2 ? lsign : sb;
-                    const C ca = cconj(A), cb = cconj(B);
-                    const C q = csub(cmul(wa, mkc(qa * ca.x, qa * ca.y)), cmul(wb, mkc(qb * cb.x, qb * cb.y)));
+                    const C qv = (p == 0 && r == R1 / 2) ? mkc(kv.x, -kv.y) : mkc(-kv.x, kv.y);
+                    const C q = csub(cmul(wa, v1 ? qv : qka), cmul(wb, v2 ? qv : qkb));
                     u = edge ? mkc((T)0.5 * (u.x + q.x), (T)0.5 * (u.y + q.y)) : q;
                 }
                 v[r] = cscale(u, r < R1 / 2 ? gs[k] : gs[L - k]);
