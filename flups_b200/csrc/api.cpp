@@ -144,7 +144,10 @@ void flups_set_greenType(Solver* s, const FLUPS_GreenType type) {
     s->green_type = type;
 }
 
-void flups_set_stream(Solver* s, void* stream) { s->stream = (cudaStream_t)stream; }
+void flups_set_stream(Solver* s, void* stream) {
+    s->stream = (cudaStream_t)stream;
+    s->cs_follows = false;
+}
 
 void flups_setup(Solver* s, const bool changeComm) {
     (void)changeComm;

@@ -157,6 +157,8 @@ extern "C" int flups_b200_solve_group(Solver* const* ss, int n, double* const* f
         for (int i = 0; i < n; ++i) gg.gens.push_back(ss[i]->gen);
         it = g_groups.emplace(key, gg).first;
     }
+    // the members' next host-array solves wait for the caller's stream again
+    for (int i = 0; i < n; ++i) ss[i]->cs_follows = false;
     const cudaError_t e = cudaGraphLaunch(it->second.exec, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
         for (int i = 0; i < n; ++i) ss[i]->last_error = (int)e;

@@ -144,6 +144,17 @@ struct Solver {
     size_t stage_out_elems = 0;
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
     cudaEvent_t ev_in[kSlabs] = {}, ev_fwd[kSlabs] = {}, ev_bwd[kSlabs] = {}, ev_out[kSlabs] = {};
+    // async host-array solves run their passes on cstream: the caller's
+    // stream waits for each solve's last download, and the next such solve
+    // need not (cs_follows: the solver's last work was such a solve, so its
+    // passes are ordered behind the previous ones on cstream already)
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_entry = nullptr;
+    bool cs_follows = false;
+    // host range [dl_lo, dl_hi) that the last streamed download writes (its
+    // slabs finish at ev_out): a later upload reading it waits for them
+    const char* dl_lo = nullptr;
+    const char* dl_hi = nullptr;
     int slab_dim = -1, slab_lo = 0, slab_hi = 0;   // restriction run_pass applies to non-fused passes
     double* inner = nullptr;              // spectral buffer of the advanced API (doubles)
     Topology* topo_spec = nullptr;
@@ -279,7 +290,7 @@ struct Solver {
     void do_backward(double* user_out, int type, int nbatch);
     void do_fft_backward_fused(double* user_out, int type, int nbatch);
     bool streamed_ok() const;
-    void solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch);
+    void solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch, bool follows);
     void restrict_slab(flb::PassArgs& A, bool in_f64, bool out_f64) const;
     // one rank's steps of a z-slab decomposed solve (flups_b200_slab_*): the
     // x and y passes of user planes [z0, z1), the last-direction pass of

@@ -264,9 +264,10 @@ Solver::~Solver() {
     }
     if (capture_stream) cudaStreamDestroy(capture_stream);
     if (h2d_stream) {
-        // copies of an async solve may still be in flight
+        // copies and passes of an async solve may still be in flight
         cudaStreamSynchronize(h2d_stream);
         cudaStreamSynchronize(d2h_stream);
+        if (cstream) cudaStreamSynchronize(cstream);
     }
     for (auto& b : buf)
         if (b) cudaFree(b);
@@ -288,6 +289,8 @@ Solver::~Solver() {
         }
         cudaStreamDestroy(h2d_stream);
         cudaStreamDestroy(d2h_stream);
+        if (cstream) cudaStreamDestroy(cstream);
+        if (ev_entry) cudaEventDestroy(ev_entry);
     }
     if (inner) cudaFree(inner);
     for (auto e : ev) cudaEventDestroy(e);
@@ -1255,6 +1258,7 @@ void Solver::compute_green() {
 
 // ---------------------------------------------------------------- setup / solve
 void Solver::setup() {
+    cs_follows = false;
     FLB_CHECK(!is_setup, "setup was already called");
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
@@ -1528,13 +1532,15 @@ void Solver::solve(double* field, double* rhs, int type, int nbatch) {
     FLB_CHECK(rhs != nullptr, "rhs is NULL");
     FLB_CHECK(nbatch >= 1, "nbatch must be >= 1");
     FLB_CHECK(!owned(), "this solver holds one rank's share of the planes: use the flups_b200_slab_* steps");
+    const bool follows = cs_follows;
+    cs_follows = false;
     ensure_buffers(nbatch);
     if (autotune) autotune_passes(type, nbatch);
     const size_t user_elems = topo_phys->memsize() * (size_t)nbatch;
     // (a solve being captured has device arrays, checked before the capture)
     const bool dev_in = capturing || is_device_ptr(rhs), dev_out = capturing || is_device_ptr(field);
     if ((!dev_in || !dev_out) && streamed_ok()) {
-        solve_streamed(field, rhs, !dev_in, !dev_out, type, nbatch);
+        solve_streamed(field, rhs, !dev_in, !dev_out, type, nbatch, follows);
         return;
     }
     double* din = rhs;
@@ -1581,7 +1587,7 @@ bool Solver::streamed_ok() const {
     return !timing && ndim == 3 && fwd[ndim - 1].dim == 2 && st[0].n[2] >= 2;
 }
 
-void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch) {
+void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_host, int type, int nbatch, bool follows) {
     const int d = 2;
     const int nd = st[0].n[d];
     const int ns = std::min(kSlabs, nd);
@@ -1608,17 +1614,50 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
             check_cuda(cudaEventCreateWithFlags(&ev_out[k], cudaEventDisableTiming), "event");
         }
     }
+    // async solves of host arrays in and out: the passes on cstream, which
+    // follows the caller's stream unless this solver's last work was such a
+    // solve (then the caller's stream ends in that solve's download wait, which
+    // the passes need not wait for: back-to-back solves overlap one's download
+    // with the next one's passes, and the copy engines never idle)
+    const cudaStream_t caller = stream;
+    const bool own = async && in_host && out_host && !capturing;
+    if (own) {
+        if (!cstream) {
+            check_cuda(cudaStreamCreateWithFlags(&cstream, cudaStreamNonBlocking), "pass stream");
+            check_cuda(cudaEventCreateWithFlags(&ev_entry, cudaEventDisableTiming), "event");
+        }
+        if (!follows) {
+            check_cuda(cudaEventRecord(ev_entry, caller), "event record");
+            check_cuda(cudaStreamWaitEvent(cstream, ev_entry, 0), "stream wait");
+        }
+        stream = cstream;
+    }
+    struct Restore {
+        cudaStream_t& s;
+        cudaStream_t keep;
+        ~Restore() { s = keep; }
+    } restore{stream, caller};
     int64_t ustr[3], ucstr;
     set_strides_user(ustr, ucstr);
     const int ncomp = lda * nbatch;
     double* din = in_host ? stage_in : rhs;
     double* dout = out_host ? stage_out : field;
+    // an rhs that an earlier solve's download writes (a chain of async solves,
+    // in place or field -> rhs): each slab's upload waits for that slab's
+    // download when the arrays coincide, the first upload for all of them when
+    // they only overlap
+    const char* r_lo = reinterpret_cast<const char*>(rhs);
+    const char* r_hi = r_lo + user_elems * sizeof(double);
+    const bool after_dl = in_host && dl_lo && r_lo < dl_hi && dl_lo < r_hi;
+    const bool per_slab = after_dl && r_lo == dl_lo;
+    if (after_dl && !per_slab) check_cuda(cudaStreamWaitEvent(h2d_stream, ev_out[ns - 1], 0), "stream wait");
     pass_idx = 0;
     for (int k = 0; k < ns; ++k) {
         const int lo = (int)((int64_t)k * nd / ns), hi = (int)((int64_t)(k + 1) * nd / ns);
         if (in_host) {
             // the previous solve's passes have read this slab of the staging array
             check_cuda(cudaStreamWaitEvent(h2d_stream, ev_fwd[k], 0), "stream wait");
+            if (per_slab) check_cuda(cudaStreamWaitEvent(h2d_stream, ev_out[k], 0), "stream wait");
             for (int c = 0; c < ncomp; ++c) {
                 const size_t off = (size_t)c * ucstr + (size_t)lo * ustr[d];
                 check_cuda(cudaMemcpyAsync(stage_in + off, rhs + off, (size_t)(hi - lo) * ustr[d] * sizeof(double),
@@ -1657,10 +1696,17 @@ void Solver::solve_streamed(double* field, double* rhs, bool in_host, bool out_h
             check_cuda(cudaEventRecord(ev_out[k], d2h_stream), "event record");
         }
     }
-    // work queued later on the caller's stream sees the downloaded result
+    stream = caller;
+    if (out_host) {
+        dl_lo = reinterpret_cast<const char*>(field);
+        dl_hi = dl_lo + user_elems * sizeof(double);
+    }
+    // work queued later on the caller's stream sees the downloaded result (and,
+    // through it, the passes)
     if (out_host) check_cuda(cudaStreamWaitEvent(stream, ev_out[ns - 1], 0), "stream wait");
     if (!async) check_cuda(cudaStreamSynchronize(stream), "solve");
     else check_cuda(cudaGetLastError(), "solve");
+    cs_follows = own;
 }
 
 // ---------------------------------------------------------------- z-slab decomposition
@@ -1868,6 +1914,7 @@ void Solver::inner_spec_strides(int64_t str[3], int64_t& cstr) const {
 }
 
 void Solver::adv_copy(const Topology* topo, double* data, int sign) {
+    cs_follows = false;
     FLB_CHECK(data != nullptr, "data is NULL");
     FLB_CHECK(topo != nullptr && topo->lda == lda, "the solver lda = %d must match the topology one", lda);
     FLB_CHECK(topo->memsize() == topo_phys->memsize(), "the topology must be the solver's physical topology");
@@ -1881,6 +1928,7 @@ void Solver::adv_copy(const Topology* topo, double* data, int sign) {
 }
 
 void Solver::adv_fft(double* data, int sign) {
+    cs_follows = false;
     FLB_CHECK(data != nullptr, "data is NULL");
     FLB_CHECK(!owned(), "this solver holds one rank's share of the planes: use the flups_b200_slab_* steps");
     FLB_CHECK(sign == FLUPS_FORWARD || sign == FLUPS_BACKWARD || sign == FLUPS_BACKWARD_DIFF, "unknown sign %d", sign);
@@ -1939,6 +1987,7 @@ void Solver::adv_fft(double* data, int sign) {
 }
 
 void Solver::adv_mult(double* data, int type) {
+    cs_follows = false;
     FLB_CHECK(data != nullptr, "data is NULL");
     FLB_CHECK(type == STD || (type == ROT && lda == 3 && odiff != NOD), "ROT needs lda = 3 and a derivative order");
     ensure_inner();
@@ -2029,6 +2078,7 @@ void Solver::autotune_passes(int type, int nbatch) {
 int Solver::solve_graph(double* field, double* rhs, int type, int nbatch) {
     if (!is_setup || !field || !rhs || nbatch < 1 || owned()) return -1;
     if (!is_device_ptr(field) || !is_device_ptr(rhs)) return -2;
+    cs_follows = false;
     GraphKey k{field, rhs, nbatch, type};
     auto it = graphs.find(k);
     if (it == graphs.end()) {

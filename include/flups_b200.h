@@ -38,9 +38,14 @@ void flups_solve_batch(struct Solver* s, double* field, double* rhs, int nbatch,
  * download of field run on the library's copy streams in slabs, overlapped
  * with the transforms and with the copies of the previous and next solve;
  * rhs and field must stay untouched until the solve is complete (for host
- * arrays page-locked memory lets the copies run asynchronously).  Completion
- * is ordered before later work on the solver's stream; flups_synchronize
- * waits for it.  Default 0 (every call returns with its result in place). */
+ * arrays page-locked memory lets the copies run asynchronously), and a host
+ * rhs must hold its values when the call is made (its upload does not wait
+ * for other work on the stream; it does wait for an earlier solve's download
+ * into the same memory, so chained and in-place calls are safe).  Solves of
+ * host arrays in and out run their transforms on a library stream, so one
+ * solve's download overlaps the next one's transforms.  Completion is
+ * ordered before later work on the solver's stream; flups_synchronize waits
+ * for it.  Default 0 (every call returns with its result in place). */
 void flups_set_async(struct Solver* s, int async);
 
 /* Wait for every solve queued on the solver's stream (async mode). */

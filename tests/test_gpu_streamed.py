@@ -95,3 +95,45 @@ def test_host_rot_equals_device():
     out = np.zeros_like(u)
     s.solve(out, u, 1)
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("name,nglob,lda,bcv,center,kernel,precision", CASES[:3], ids=[c[0] for c in CASES[:3]])
+def test_host_async_chain(name, nglob, lda, bcv, center, kernel, precision):
+    """Async solves of pinned host arrays whose rhs is an earlier solve's field
+    (in place, then field -> rhs), with device-array solves (plain and graph)
+    queued between them on the same stream: after one synchronize every result
+    equals the same chain run one device solve at a time."""
+    import torch
+    t, s = _setup(nglob, lda, bcv, center, kernel, precision)
+    rng = np.random.default_rng(11)
+    u0 = to_user(rng.standard_normal((lda,) + tuple(nglob)))
+    ud = to_user(rng.standard_normal((lda,) + tuple(nglob)))
+    r1 = _device_solve(s, u0)
+    r2 = _device_solve(s, r1)
+    r3 = _device_solve(s, r2)
+    r4 = _device_solve(s, r3)
+    rd = _device_solve(s, ud)
+    h1 = torch.from_numpy(u0.copy()).pin_memory()
+    h2 = torch.full_like(h1, float("nan")).pin_memory()
+    h3 = torch.full_like(h1, float("nan")).pin_memory()
+    d_in = torch.from_numpy(ud).cuda()
+    d_out = torch.zeros_like(d_in)
+    g_out = torch.zeros_like(d_in)
+    s.solve_graph(g_out, d_in)      # first call: plain solve + capture
+    torch.cuda.synchronize()
+    g_out.zero_()
+    s.set_async(True)
+    s.solve(h1, h1)                 # h1 = S(u0), in place
+    s.solve(h1, h1)                 # h1 = S(S(u0)), in place again
+    s.solve(d_out, d_in)            # a device-array solve between them
+    s.solve(h2, h1)                 # h2 = S^3(u0)
+    s.solve_graph(g_out, d_in)      # a graph replay between them
+    s.solve(h3, h2)                 # h3 = S^4(u0)
+    s.synchronize()
+    s.set_async(False)
+    assert s.last_error() == 0
+    assert np.array_equal(h1.numpy(), r2)
+    assert np.array_equal(h2.numpy(), r3)
+    assert np.array_equal(h3.numpy(), r4)
+    assert np.array_equal(d_out.cpu().numpy(), rd)
+    assert np.array_equal(g_out.cpu().numpy(), rd)
