@@ -79,12 +79,17 @@ bool make_prefetch(Prefetch& pf, const void* base, const uint64_t dims[4], const
 int fast_stage_table_len(int n, int f64) { return stage_table_entries(n, fast_radix1_of(n, f64)); }
 int fast_stage_table_len_r1(int n, int r1) { return stage_table_entries(n, r1); }
 
+#ifndef FLB_COL_HALF1
+#define FLB_COL_HALF1 1
+#endif
 cudaError_t launch_fast_col(int f64, int mode, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     auto shape = [L](int n) { return n == L ? SH_FULL : (2 * n == L ? SH_HALF : SH_ANY); };
     int sh;
     if (mode == 0) sh = (a.nout == L) ? shape(a.nin) : SH_ANY;
     else if (mode == 1) sh = (a.nin == L) ? shape(a.nout) : SH_ANY;
     else sh = (shape(a.nin) == shape(a.nout)) ? shape(a.nin) : SH_ANY;
+    // fused lines of a node-centred unbounded direction: L/2 + 1 in and out
+    if (FLB_COL_HALF1 && mode == 2 && L % 2 == 0 && 2 * a.nin == L + 2 && a.nout == a.nin) sh = SH_HALF1;
     if (mode == 3) return f64 ? launch_col_f64_m3(sh, L, a, ncomp, s) : launch_col_f32_m3(sh, L, a, ncomp, s);
     if (f64) return (mode == 2) ? launch_col_f64_m2(sh, L, a, ncomp, s) : launch_col_f64_m01(mode, sh, L, a, ncomp, s);
     if (mode == 2) return launch_col_f32_m2(sh, L, a, ncomp, s);

@@ -175,12 +175,21 @@ struct RegFFT {
     }
 
     // in place on v: forward (INV: inverse) unnormalised DFT of the line held as
-    // v[r] = x[p + P r]; ZIN: x is zero from L/2 on (v[r] = 0 for r >= R1/2)
-    template <bool ZIN, bool INV>
-    __device__ static __forceinline__ void fft(C* v, C* sm, int p, const C* __restrict__ tws) {
+    // v[r] = x[p + P r]; ZIN: x is zero from L/2 on (v[r] = 0 for r >= R1/2);
+    // Z1 (with ZIN): but for x_{L/2} = xh, held by lane 0 only, whose share of
+    // lane 0's first-radix outputs is W_R1^{(R1/2) k} xh = (-1)^k xh
+    template <bool ZIN, bool INV, bool Z1 = false>
+    __device__ static __forceinline__ void fft(C* v, C* sm, int p, const C* __restrict__ tws, C xh = C{}) {
         static_assert(!(ZIN && INV), "zero-padded inputs are forward transforms here");
+        static_assert(!Z1 || ZIN, "x_{L/2} alone is added to a zero-padded line");
         if constexpr (ZIN) dftz<R1>(v);
         else dftr<R1, INV>(v);
+        if constexpr (Z1) {
+            if (p == 0) {
+#pragma unroll
+                for (int k = 0; k < R1; ++k) v[k] = (k & 1) ? csub(v[k], xh) : cadd(v[k], xh);
+            }
+        }
         if constexpr (P > 1) {
             line_sync<WSYNC>();
             // sw(p R1 + k) = sw(p R1) + k for k < R1 when R1 divides 32
@@ -380,7 +389,9 @@ struct Occ {
 
 // ---------------------------------------------------------------- columns
 // Extent of the loaded / stored part of a line, known at compile time:
-enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2 };  // tested per element, L/2, L
+// tested per element, L/2, L; L/2 + 1 (the zero-padded line of a node-centred
+// unbounded direction: n nodes in a 2 (n - 1)-point line; fused passes only)
+enum { SH_ANY = 0, SH_HALF = 1, SH_FULL = 2, SH_HALF1 = 3 };
 // MODE 0: forward DFT (SH: loaded part; SH != ANY also means all L stored),
 //      1: inverse DFT (SH: stored part; SH != ANY also means all L loaded),
 //      2: forward, Green multiply, inverse (SH: loaded and stored part).
@@ -391,8 +402,10 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     using C = typename CT<T>::C;
     constexpr int INS = (MODE == 1) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
     constexpr int OUTS = (MODE == 0) ? (SH == SH_ANY ? SH_ANY : SH_FULL) : SH;
-    constexpr int NLD = (INS == SH_HALF) ? R1 / 2 : R1;  // registers loaded
-    constexpr int NST = (OUTS == SH_HALF) ? R1 / 2 : R1;  // registers stored
+    static_assert(SH != SH_HALF1 || MODE == 2, "L/2 + 1 lines are fused passes");
+    constexpr bool ZH = INS == SH_HALF || INS == SH_HALF1;
+    constexpr int NLD = ZH ? R1 / 2 : R1;  // registers loaded
+    constexpr int NST = (OUTS == SH_HALF || OUTS == SH_HALF1) ? R1 / 2 : R1;  // registers stored
     extern __shared__ __align__(16) unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
     const int c = threadIdx.x % TX, p = threadIdx.x / TX;
@@ -431,6 +444,11 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
             v[r] = ok ? t : mkc((T)0, (T)0);
         }
     }
+    // x_{L/2} of an L/2 + 1 line: lane 0's register R1/2
+    C xh = mkc((T)0, (T)0);
+    if constexpr (INS == SH_HALF1) {
+        if (p == 0) xh = in[(R1 / 2) * ls];
+    }
     // the table's copies are complete before the first exchange's barrier
     if constexpr (F::TWS) {
         if constexpr (MODE == 2) cp_async_wait<1>();
@@ -438,7 +456,7 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
     }
     C* line = sm + c * F::SC;
     if constexpr (MODE == 1) F::template fft<false, true>(v, line, p, tws);
-    else F::template fft<INS == SH_HALF, false>(v, line, p, tws);
+    else F::template fft<ZH, false, INS == SH_HALF1>(v, line, p, tws, xh);
     if constexpr (MODE == 2) {
         cp_async_wait_all();
         __syncthreads();
@@ -468,6 +486,9 @@ __global__ void __launch_bounds__(TX * (L / R1), (Occ<TX * (L / R1), MODE == 2, 
 #pragma unroll
         for (int r = 0; r < NST; ++r) {
             if (OUTS != SH_ANY || p + F::P * r < a.nout) out[r * os] = v[r];
+        }
+        if constexpr (OUTS == SH_HALF1) {
+            if (p == 0) out[(R1 / 2) * os] = v[R1 / 2];
         }
     }
 }
@@ -1856,6 +1877,8 @@ template <typename T, int MODE>
 inline cudaError_t launch_col_shape(int sh, int L, const ColArgs& a, int ncomp, cudaStream_t s) {
     if (sh == SH_FULL) return launch_col_mode<T, MODE, SH_FULL>(L, a, ncomp, s);
     if (sh == SH_HALF) return launch_col_mode<T, MODE, SH_HALF>(L, a, ncomp, s);
+    if constexpr (MODE == 2)
+        if (sh == SH_HALF1) return launch_col_mode<T, MODE, SH_HALF1>(L, a, ncomp, s);
     return launch_col_mode<T, MODE, SH_ANY>(L, a, ncomp, s);
 }
 
