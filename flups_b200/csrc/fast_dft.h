@@ -140,6 +140,17 @@ __host__ __device__ constexpr int fast_radix1_row(int n, int f64) {
 __host__ __device__ constexpr int fast_radix1_mode(int n, int f64, int mode) {
     return (mode < 2 && fast_radix48(n, f64)) ? 48 : ((n % 3 != 0) ? fast_radix1_of(n, 0) : fast_radix1_of(n, f64));
 }
+// the real-side columns (col_real_kernel, col_real_pair_kernel): FP32
+// power-of-two lines from 128 to FLB_COLREAL_R16_MAX points take a first radix
+// of 16 (half the registers of 32, four 256-thread CTAs per SM), else the
+// default (256-point y columns of the 513 x 257 x 257 node grid: r2c 73.6 ->
+// 64.6 us, c2r 68.1 -> 66.7 us; the 64 x 128^3 batch 3.19 -> 3.05 ms)
+#ifndef FLB_COLREAL_R16_MAX
+#define FLB_COLREAL_R16_MAX 256
+#endif
+__host__ __device__ constexpr int fast_radix1_colreal(int n, int f64) {
+    return (!f64 && n % 3 != 0 && n >= 128 && n <= FLB_COLREAL_R16_MAX) ? 16 : fast_radix1_of(n, f64);
+}
 // the fused ROT rows (row_rot_kernel): FP32 384- and 768-point lines with a first
 // radix of 48 (two Stockham stages, one exchange per DFT instead of two; 168
 // registers, 28 bytes spilled), else the fused passes' radix

@@ -929,7 +929,9 @@ inline cudaError_t launch_row_fused_shape(int sh, int L, const RowFusedArgs& a, 
 #endif
 template <typename T, int R1, bool C2R, int THREADS>
 struct ColRealOcc {
-    static constexpr int dflt = (sizeof(T) == 4 && !C2R && R1 <= 24 && THREADS == 256) ? 3 : Occ<THREADS>::blocks;
+    static constexpr int dflt = (sizeof(T) == 4 && R1 <= 16 && THREADS == 256)
+                                    ? 4
+                                    : ((sizeof(T) == 4 && !C2R && R1 <= 24 && THREADS == 256) ? 3 : Occ<THREADS>::blocks);
     static constexpr int blocks =
         FLB_COLREAL_PER_SM > 0 ? (FLB_COLREAL_PER_SM / THREADS > 0 ? FLB_COLREAL_PER_SM / THREADS : 1) : dflt;
 };
@@ -1394,6 +1396,18 @@ struct DctOcc {
     static constexpr int blocks = over > 0 ? over : dflt;
 };
 
+// rows whose outputs need no per-element test store them from a compile-time
+// unrolled loop (0: every output through the general test; 513 x 257 x 257
+// node grid: DCT-III rows 140 -> 115 us, DCT-II rows 116 -> 107 us)
+#ifndef FLB_DCT_PLAIN_STORE
+#define FLB_DCT_PLAIN_STORE 1
+#endif
+// DCT-III rows of all N inputs pre-processed from registers and lane
+// shuffles (0: from a staged copy of the row in shared memory; the same grid:
+// 115 -> 112 us)
+#ifndef FLB_DCT3_SHFL
+#define FLB_DCT3_SHFL 1
+#endif
 template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
 __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>::blocks) row_dct_kernel(const RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
@@ -1424,6 +1438,10 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
     }
     cp_async_commit();
     const bool dst = (a.kind == LK_DST1 || a.kind == LK_DST2 || a.kind == LK_DST3 || a.kind == LK_DST4);
+    // DCT-III rows of all N inputs: pre-processed from registers and lane
+    // shuffles instead of a staged copy of the row
+    constexpr bool SHFL3 = FAM == 3 && FLB_DCT3_SHFL && P <= 32 && (P & (P - 1)) == 0;
+    T u3[SHFL3 ? 2 * R1 : 1];
     // inputs the transform reads: n (DCT-I n = LH + 1, DST-I n = LH - 1), else up to N
     const int ntr = (FAM == 1) ? a.n : N;
     const int nld = valid ? (a.nin - a.fi < ntr ? a.nin - a.fi : ntr) : 0;
@@ -1486,6 +1504,10 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
             lr[slot(LH)] = u;  // DCT-I: x_LH; DST-I: z_LH = 0
             if (dst) lr[slot(0)] = z;
         }
+    } else if (SHFL3 && !dst && nld >= N) {
+        // DCT-III rows held in registers: u[r] = x_{p + P r}
+#pragma unroll
+        for (int r = 0; r < 2 * R1; ++r) u3[r] = (T)src[p + P * r];
     } else {
         // rows that hold all N inputs load them without a test per element
         if (nld >= N) stage(std::true_type{});
@@ -1506,6 +1528,31 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
         for (int r = 0; r < R1; ++r) {
             const int j = p + P * r;
             v[r] = cmul(cmul(line[F::sw(j)], w4[2 * j]), w8);
+        }
+    } else if (SHFL3 && !dst && nld >= N) {
+        // x_k = u[r] and x_{LH+k} = u[r + R1] are this lane's (k = p + P r); for
+        // p > 0, x_{N-k} and x_{LH-k} are lane P - p's u[2 R1 - 1 - r] and
+        // u[R1 - 1 - r]; lane 0 holds its own (x_N = 0)
+        const int lane = threadIdx.x & 31;
+        const unsigned gm = (P >= 32) ? 0xffffffffu : (((1u << (P & 31)) - 1u) << (lane & ~(P - 1)));
+        const int src_lane = (P - p) & (P - 1);
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+            const int k = p + P * r;
+            const T sn = __shfl_sync(gm, u3[2 * R1 - 1 - r], src_lane, P);
+            const T sl = __shfl_sync(gm, u3[R1 - 1 - r], src_lane, P);
+            const T xn = (p == 0) ? (r == 0 ? z : u3[(2 * R1 - r) % (2 * R1)]) : sn;
+            const T xl = (p == 0) ? u3[R1 - r] : sl;
+            C xk = cmulc(mkc(u3[r], -xn), w4[k]);
+            C xm = cmulc(mkc(xl, -u3[r + R1]), w4[LH - k]);
+            if (k == 0) {
+                xk.y = z;
+                xm.y = z;
+            }
+            xm = cconj(xm);
+            const C A = cadd(xk, xm);
+            const C B = cmul(csub(xk, xm), cconj(wn[k]));
+            v[r] = mkc(A.x - B.y, A.y + B.x);
         }
     } else {
         auto x = [&](int i) { return (i >= 0 && i < N) ? lr[slot(i)] : z; };
@@ -1616,8 +1663,20 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
         else y = outv(i);
         out[i] = (OT)y;
     };
-    if constexpr (FAM == 3) {
+    // the usual row: transform outputs from index 0, all N of them stored, no
+    // period copy and no nulled output among them but (maybe) output 0
+    const bool plain = FAM != 1 && FLB_DCT_PLAIN_STORE && a.fo == 0 && !period && a.nstore >= N && (!last || a.ilast >= N);
+    if (plain) {
         // outputs i < N as p + P r (compile-time r), then the rest
+#pragma unroll
+        for (int r = 0; r < 2 * R1; ++r) {
+            const int i = p + P * r;
+            T y = value(i);
+            if (r == 0 && first && p == 0) y = z;
+            out[i] = (OT)y;
+        }
+        for (int i = N + p; i < a.nstore; i += P) store(i);
+    } else if constexpr (FAM == 3) {
 #pragma unroll
         for (int r = 0; r < 2 * R1; ++r) {
             const int i = p + P * r;
@@ -1825,7 +1884,7 @@ inline cudaError_t launch_rot_shape(int sh, int L, const ColArgs& a, int ncomp, 
 
 template <typename T, typename RT, int L, bool C2R, int SH>
 inline cudaError_t launch_colreal_t(const ColArgs& a, int ncomp, cudaStream_t s) {
-    constexpr int R1 = fast_radix1_of(L, sizeof(T) == 8);
+    constexpr int R1 = fast_radix1_colreal(L, sizeof(T) == 8);
     constexpr int TX = (L == 512 ? 128 : 256) / (L / R1);
     static_assert(TX >= 1, "tile narrower than one column");
     using F = RegFFT<T, L, R1>;

@@ -157,7 +157,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
         } else if (kinds[i] == 1) {
             slot_for(A.st[0].M, fast_radix1_mode(A.st[0].M, f64 ? 1 : 0, A.fused ? 2 : 0));
         } else if (kinds[i] == 3) {
-            slot_for(A.st[0].M, r1_of(A.st[0].M));
+            slot_for(A.st[0].M, fast_radix1_colreal(A.st[0].M, f64 ? 1 : 0));
         } else if (kinds[i] == 5) {
             const int M = A.st[0].M;
             slot_for(M, A.mult.mode == 2 ? fast_radix1_rowrot(M, f64 ? 1 : 0) : fast_radix1_rowfused(M, f64 ? 1 : 0));
@@ -219,7 +219,7 @@ extern "C" int flups_solve_noalloc(Solver* s, double* field, double* rhs, int ty
                     c.tws = tw_of(L, fast_radix1_mode(L, f64 ? 1 : 0, mode));
                     if (go) e = launch_fast_col(f64 ? 1 : 0, mode, L, c, A.ncomp, st);
                 } else if (kinds[i] == 3) {
-                    c.tws = tw_of(L, r1_of(L));
+                    c.tws = tw_of(L, fast_radix1_colreal(L, f64 ? 1 : 0));
                     if (go) e = launch_fast_colreal(f64 ? 1 : 0, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, st);
                 } else if (kinds[i] == 4) {
                     r.tw2 = tw_of(2 * L, 0);

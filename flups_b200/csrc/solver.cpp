@@ -795,7 +795,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         return;
     }
     if (kind == 3) {
-        c.tws = stage_table(L, f64);
+        c.tws = stage_table(L, f64, fast_radix1_colreal(L, f64 ? 1 : 0));
         check_cuda(launch_fast_colreal(f64, A.st[0].spec[0].kind == LK_C2R, L, c, A.ncomp, stream), "column r2c/c2r launch");
         return;
     }
