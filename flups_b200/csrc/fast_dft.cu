@@ -31,6 +31,11 @@ int fast_row_tile_rows(int f64, int L) {
     return p >= threads ? 1 : threads / p;
 }
 
+int fast_rowrot_rows(int f64, int L) {
+    const int p = L / fast_radix1_rowrot(L, f64);
+    return p > 32 ? 0 : FLB_ROWROT_TRIPLES * (32 / p);
+}
+
 int fast_col_tile_width(int f64, int L, int tile) {
     const int r1 = fast_radix1_mode(L, f64, 0);
     return col_tile_threads(L, tile, (f64 && L % 3 != 0) || r1 == 48) / (L / r1);

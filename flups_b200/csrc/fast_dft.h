@@ -76,6 +76,9 @@ struct RowFusedArgs {
     int kstr;
     int ax1, ax2;
     int nyq[3];
+    // L2 prefetch of a later block's rows (ROT rows; nbox = 0: none).  Map
+    // dims: 8-byte units along the row, i1, i2, component
+    Prefetch pf;
 };
 
 struct RowArgs {
@@ -112,6 +115,8 @@ bool fast_col_supported(int L);
 int fast_col_tile_width(int f64, int L, int tile);
 // rows per CTA of the r2c / c2r row pass of real length L
 int fast_row_tile_rows(int f64, int L);
+// row positions per block of the fused ROT rows
+int fast_rowrot_rows(int f64, int L);
 bool fast_row_supported(int L);
 
 // First radix of the register DFTs for an n-point line: 32 in FP32 and 16 in

@@ -742,6 +742,17 @@ __global__ void __launch_bounds__(NT * 96, RowFusedOcc<T>::per_sm / (NT * 96) > 
     const int p = lane % P, lw = lane / P;
     const int64_t row = (int64_t)blockIdx.x * (NT * LPW) + tri * LPW + lw;  // row position
     const bool valid = row < (int64_t)a.n1 * a.n2;
+    if (a.pf.nbox > 0 && threadIdx.x == 0) {
+        // the rows of the block pf.dist launches ahead (x, then y order), into L2
+        const long long lin = blockIdx.x + (long long)gridDim.x * blockIdx.y + a.pf.dist;
+        const int bx = (int)(lin % gridDim.x), by = (int)(lin / gridDim.x);
+        if (by < (int)gridDim.y) {
+            const int64_t row0 = (int64_t)bx * (NT * LPW);
+            const int p1 = (int)(row0 % a.n1), p2 = (int)(row0 / a.n1);
+            for (int gg = 0; gg < 3; ++gg)
+                for (int k = 0; k < a.pf.nbox; ++k) l2_prefetch_box(&a.pf.map, k * a.pf.step, p1, p2, 3 * by + gg);
+        }
+    }
     const int i1 = valid ? (int)(row % a.n1) : 0, i2 = valid ? (int)(row / a.n1) : 0;
     const int comp = 3 * blockIdx.y + g;
     // lines of the triple: [component][lw]; Green's rows of the triple after all lines

@@ -281,6 +281,7 @@ struct Solver {
     bool prefetch = true;
     void col_prefetch(flb::ColArgs& c, bool f64, int L, int ncomp) const;
     void row_prefetch(flb::RowArgs& r, bool f64, bool c2r, int L, int ncomp) const;
+    void rowrot_prefetch(flb::RowFusedArgs& f, bool f64, int L, int ncomp) const;
     static constexpr int kOvSlabs = 4;
     cudaStream_t ov_stream[2] = {nullptr, nullptr};
     cudaEvent_t ov_ev0 = nullptr, ov_evf[kOvSlabs] = {}, ov_evg[kOvSlabs] = {};

@@ -775,6 +775,7 @@ void Solver::launch_fast(const PassArgs& A, int kind, bool f64, bool in_f64, boo
         RowFusedArgs f;
         rowfused_args(A, f);
         f.tws = stage_table(L, f64, A.mult.mode == 2 ? fast_radix1_rowrot(L, f64 ? 1 : 0) : fast_radix1_rowfused(L, f64 ? 1 : 0));
+        if (prefetch && A.mult.mode == 2) rowrot_prefetch(f, f64, L, A.ncomp);
         check_cuda(launch_fast_rowfused(f64 ? 1 : 0, A.mult.mode == 2, L, f, A.ncomp, stream), "fused row launch");
         return;
     }
@@ -857,6 +858,25 @@ void Solver::row_prefetch(RowArgs& r, bool f64, bool c2r, int L, int ncomp) cons
     const uint64_t strides[3] = {(uint64_t)r.in_s1 * elem, s2, ncomp > 1 ? (uint64_t)r.in_cstr * elem : s2 * n2};
     const uint32_t box[4] = {(uint32_t)std::min<uint64_t>(256, (units + 1) / 2 * 2), (uint32_t)std::min(tr, r.n1), 1, 1};
     make_prefetch(r.pf, r.in, dims, strides, box, (int)((units + 255) / 256), 256, PREFETCH_DIST);
+}
+
+// the ROT rows run two CTAs per SM: the block one wave of resident blocks
+// ahead starts as this one ends, so its rows are fetched into L2 meanwhile
+#ifndef FLB_ROWROT_PREFETCH
+#define FLB_ROWROT_PREFETCH 1
+#endif
+void Solver::rowrot_prefetch(RowFusedArgs& f, bool f64, int L, int ncomp) const {
+    const int rows = fast_rowrot_rows(f64 ? 1 : 0, L);
+    const uint64_t elem = f64 ? 16 : 8;
+    const uint64_t row_bytes = (uint64_t)f.nin * elem;
+    if (!FLB_ROWROT_PREFETCH || rows == 0 || (double)row_bytes * f.n1 * f.n2 * ncomp < PREFETCH_MIN_BYTES) return;
+    const uint64_t units = (row_bytes + 7) / 8;
+    const uint64_t n2 = (uint64_t)f.n2;
+    const uint64_t s2 = (uint64_t)f.s2 * elem;
+    const uint64_t dims[4] = {units, (uint64_t)f.n1, n2, (uint64_t)ncomp};
+    const uint64_t strides[3] = {(uint64_t)f.s1 * elem, s2, ncomp > 1 ? (uint64_t)f.cstr * elem : s2 * n2};
+    const uint32_t box[4] = {(uint32_t)std::min<uint64_t>(256, (units + 1) / 2 * 2), (uint32_t)std::min(rows, f.n1), 1, 1};
+    make_prefetch(f.pf, f.in, dims, strides, box, (int)((units + 255) / 256), 256, 2 * 148);
 }
 
 const void* Solver::stage_table(int n, bool f64, int r1) {
