@@ -1419,6 +1419,18 @@ struct DctOcc {
 #ifndef FLB_DCT3_SHFL
 #define FLB_DCT3_SHFL 1
 #endif
+// line stride of the DCT rows (complex elements): FP32 rows of 16 lanes share
+// a warp two by two, and at F::SC (a multiple of 16) the second row's 4-byte
+// accesses (the packed scatter, the output gather) hit the first row's banks;
+// FLB_DCT_SC_PAD complex elements more put them 8 banks apart
+#ifndef FLB_DCT_SC_PAD
+#define FLB_DCT_SC_PAD 4
+#endif
+template <typename F, typename T>
+struct DctSC {
+    static constexpr int V = F::SC + ((sizeof(T) == 4 && F::P == 16) ? FLB_DCT_SC_PAD : 0);
+};
+
 template <typename T, typename IT, typename OT, int LH, int R1, int TR, int FAM>
 __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>::blocks) row_dct_kernel(const RowArgs a) {
     using F = RegFFT<T, LH, R1, true>;
@@ -1435,10 +1447,11 @@ __global__ void __launch_bounds__(TR * (LH / R1), DctOcc<T, R1, TR * (LH / R1)>:
     // src0: the row; src: the transform's first input (fi into the row)
     const IT* src0 = reinterpret_cast<const IT*>(a.in) + comp * a.in_cstr + (int64_t)i1 * a.in_s1 + (int64_t)i2 * a.in_s2;
     const IT* src = src0 + a.fi;
-    C* line = sm + rr * F::SC;
+    constexpr int SCD = DctSC<F, T>::V;
+    C* line = sm + rr * SCD;
     T* lr = reinterpret_cast<T*>(line);
-    const C* tws = stage_twiddles<F>(a.tws, sm + TR * F::SC);
-    C* wsm = sm + TR * F::SC + F::TW_SMEM;
+    const C* tws = stage_twiddles<F>(a.tws, sm + TR * SCD);
+    C* wsm = sm + TR * SCD + F::TW_SMEM;
     if constexpr (WSM) stage_table_part<C, LH>(a.tw, wsm);
     // the W_4n^q of this family, staged while the row loads are in flight
     const C* w4 = reinterpret_cast<const C*>(a.tw2);
@@ -1988,7 +2001,7 @@ inline cudaError_t launch_dct_t(const RowArgs& a, int ncomp, cudaStream_t s) {
     using F = RegFFT<T, LH, R1, true>;
     constexpr int TR = (F::P >= 256) ? 1 : 256 / F::P;
     const size_t smem =
-        (size_t)(TR * F::SC + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0) + DctW4<T, FAM, LH>::N) * sizeof(typename CT<T>::C);
+        (size_t)(TR * DctSC<F, T>::V + F::TW_SMEM + (FAM != 4 ? RowTw<T, LH>::N : 0) + DctW4<T, FAM, LH>::N) * sizeof(typename CT<T>::C);
     static std::atomic<unsigned long long> attr{0};
     if (cudaError_t e = smem_attr_once(attr, row_dct_kernel<T, IT, OT, LH, R1, TR, FAM>, smem); e != cudaSuccess) return e;
     dim3 grid((a.nrows + TR - 1) / TR, ncomp);
