@@ -9,7 +9,8 @@ lengths in one direction and short lines in the others, so the oracle (FP64
 numpy, the reference's FFTW calls of src/FFTW_plan_dim.cpp:681-716) finishes
 in seconds.  The same is done for the longest lines the register DFTs take
 (4096-point rows, 2048-point columns, 3 x 2^k up to 3072 / 1536), for the
-node-centred DCT-III / DCT-II rows of n = 512 (513 x 257 x 257 workload), for
+node-centred DCT-III / DCT-II rows of n = 512 and the fused z pass of 257
+nodes in 512-point lines (513 x 257 x 257 workload), for
 the node-centred DCT-I / DST-I rows (EVEN/EVEN and ODD/ODD, 65 and 257
 points) and for one full 256^3 solve.  Each case also checks, through the host plan
 description, that the passes of the intended length run the register DFTs.
@@ -44,6 +45,9 @@ CASES = [
     ("xrows768_384x24x24", [384, 24, 24], UNB3, CELL_CENTER, CHAT_2, 768, 0),
     ("xrows384_192x24x24", [192, 24, 24], UNB3, CELL_CENTER, LGF_2, 384, 0),
     ("node513_dct_rows_eo_per_unb", [513, 33, 33], EO_PER_UNB, NODE_CENTER, HEJ_4, 1024, 0),
+    # the fused z pass of the same workload: 257 nodes in a 512-point line
+    # (L/2 + 1 loaded and stored)
+    ("node_fused512_eo_per_unb_17x17x257", [17, 17, 257], EO_PER_UNB, NODE_CENTER, HEJ_4, 512, 2),
     # DCT-I / DST-I rows (node-centred EVEN/EVEN, ODD/ODD): the real DFT of the
     # extension through a register DFT of half its length
     ("node257_dct1_rows_ee_per_unb", [257, 17, 17], EE_PER_UNB, NODE_CENTER, HEJ_4, 512, 0),
