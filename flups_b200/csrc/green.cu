@@ -284,6 +284,18 @@ __device__ double g_2unb1spe(const GreenEvalArgs& A, double r, double k, int i0,
     return -C_1O2PI * besselk0_d(fabs(k) * r);
 }
 
+// 1 - erf(x) as the reference forms it (src/green_kernels.hpp:469): 1 minus
+// the double nearest erf(x).
+// For x >= 2, 1 - erfc(x) rounds to that double (erfc(x) < 0.005 is known
+// far below half an ulp of 1) and the subtraction from 1 is exact, whereas
+// erf(x) itself may come out an ulp away; hej_1unb multiplies the result by
+// exp(s rho), which turns that ulp into a relative error of up to 1e-4 in a
+// Green's value (and 1e-12 - 1e-11 in a solve)
+__device__ double one_minus_erf(double x) {
+    if (x >= 2.0) return __dadd_rn(1.0, -__dadd_rn(1.0, -erfc(x)));
+    return 1.0 - erf(x);
+}
+
 __device__ double hej_1unb(int kind, double r, double k, double sig, bool zero_k) {
     const double rho = r / sig;
     const double rosqrt2 = r * C_1OSQRT2;
@@ -305,8 +317,8 @@ __device__ double hej_1unb(int kind, double r, double k, double sig, bool zero_k
     const double s = k * sig;
     const double s2 = s * s, rho2 = rho * rho;
     const double sub = (s * rho > 100.) ? 0.0
-                                        : ((1.0 - erf(C_1OSQRT2 * (s - rho))) * exp(-s * rho) +
-                                           (1.0 - erf(C_1OSQRT2 * (s + rho))) * exp(s * rho));
+                                        : (one_minus_erf(C_1OSQRT2 * (s - rho)) * exp(-s * rho) +
+                                           one_minus_erf(C_1OSQRT2 * (s + rho)) * exp(s * rho));
     const double base = -.25 * sig / s * sub;
     const double pre = sig * 1.41421356237309504880 * C_1OSQRTPI;
     const double e = exp(-.5 * (s * s + rho * rho));

@@ -48,6 +48,10 @@ CASES = [
     # the fused z pass of the same workload: 257 nodes in a 512-point line
     # (L/2 + 1 loaded and stored)
     ("node_fused512_eo_per_unb_17x17x257", [17, 17, 257], EO_PER_UNB, NODE_CENTER, HEJ_4, 512, 2),
+    # 256-point real-side columns (first radix 16): the node grid's periodic y
+    # (257 nodes) and, with device arrays, the z columns of the x-last order
+    ("node_yreal256_eo_per_unb_17x257x17", [17, 257, 17], EO_PER_UNB, NODE_CENTER, HEJ_4, 256, 1),
+    ("zreal256_32x32x128", [32, 32, 128], UNB3, CELL_CENTER, LGF_2, 256, 2),
     # DCT-I / DST-I rows (node-centred EVEN/EVEN, ODD/ODD): the real DFT of the
     # extension through a register DFT of half its length
     ("node257_dct1_rows_ee_per_unb", [257, 17, 17], EE_PER_UNB, NODE_CENTER, HEJ_4, 512, 0),
@@ -133,11 +137,6 @@ def test_kernel_instance_matches_oracle(name, nglob, bcv, center, kernel, M, axi
         fused = [p for p in plan["passes"] if p["name"] == "fused"]
         assert fused[0]["axis"] == 0 and fused[0]["fast"] == 5
     ref = _oracle(name, nglob, 1, bcv, center, kernel, rhs)
-    if precision == 64 and ("dct1" in name or "dst1" in name):
-        # these EVEN/EVEN and ODD/ODD node grids differ from the oracle by
-        # 2.4e-12 - 4.9e-12 in FP64 whichever row kernel runs (the M-point
-        # DFT of the extension gave the same figures)
-        tol = 1e-11
     assert rel_l2(got, ref) <= tol
 
 
