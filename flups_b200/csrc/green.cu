@@ -124,15 +124,45 @@ __device__ double sine_integral_d(double x) {
 }
 
 // int_0^x (1 - J0(u))/u du, Humbert's series truncated at 50 terms (double precision here)
+// double-double numbers (hi + lo, |lo| <= ulp(hi) / 2): error-free sums
+// (Knuth's two-sum) and products (an FMA gives the rounding error of hi * hi)
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_norm(double s, double e) {
+    const double hi = __dadd_rn(s, e);
+    return {hi, __dadd_rn(e, -__dadd_rn(hi, -s))};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+    const double s = __dadd_rn(a.hi, b.hi);
+    const double bb = __dadd_rn(s, -a.hi);
+    const double e = __dadd_rn(__dadd_rn(a.hi, -__dadd_rn(s, -bb)), __dadd_rn(b.hi, -bb));
+    return dd_norm(s, __dadd_rn(e, __dadd_rn(a.lo, b.lo)));
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+    const double p = __dmul_rn(a.hi, b.hi);
+    const double e = __fma_rn(a.hi, b.hi, -p);
+    return dd_norm(p, __dadd_rn(e, __dadd_rn(__dmul_rn(a.hi, b.lo), __dmul_rn(a.lo, b.hi))));
+}
+__device__ __forceinline__ DD dd_div(DD a, double b) {
+    const double q1 = __ddiv_rn(a.hi, b);
+    const DD r = dd_add(a, {-__dmul_rn(q1, b), -__fma_rn(q1, b, -__dmul_rn(q1, b))});
+    return dd_norm(q1, __ddiv_rn(r.hi, b));
+}
+
+// The same truncated series as the reference (50 terms of Humbert's
+// expansion, src/ji0.hpp:37-44), summed in double-double: its alternating
+// terms reach 1e11 at x = 30 against a sum of about 3, which leaves a double
+// sum a relative error of 1e-5 there (the reference's long double, 1e-9)
 __device__ double ji0c_d(double x) {
-    const double q = -(.25 * x * x);
-    double val = 0.0;
-    for (int n = 50; n > 0; --n) {
-        double inv_f = 1.0;
-        for (int i = 2; i <= n; ++i) inv_f /= (double)i;
-        val -= pow(q, (double)n) * inv_f * inv_f / n * .5;
+    const DD q = dd_mul({-0.25, 0.0}, dd_mul({x, 0.0}, {x, 0.0}));
+    DD t = {1.0, 0.0}, val = {0.0, 0.0};
+    for (int n = 1; n <= 50; ++n) {
+        t = dd_div(dd_mul(t, q), (double)n * (double)n);  // q^n / (n!)^2
+        const DD u = dd_div(t, 2.0 * n);
+        val = dd_add(val, {-u.hi, -u.lo});
     }
-    return val;
+    return __dadd_rn(val.hi, val.lo);
 }
 
 __device__ __forceinline__ double lgf2_symbol(double k) {
